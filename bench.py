@@ -1,0 +1,291 @@
+#!/usr/bin/env python
+"""Benchmark of the fused RQMC path kernel on the reference's headline workload.
+
+Workload (the RQMC configuration the metric is quoted on): arithmetic-average Asian call under
+GBM, S0 = K = 100, r = mu = 0.03, sigma = 0.25, T = 1, 256 Euler steps = 256 Hong–Hickernell
+scrambled Sobol dimensions, R = 32 replicas with salts 42.., raw noise ordering.
+
+  value  one "step" = one fused pass over 32 replicas x N points x 256 steps (default
+         N = 2^18 per replica, 2.1e9 path-steps), inputs (direction tables, parameters)
+         resident, sums left on the device; device time from CUDA events on the launching
+         stream; L2 flushed (256 MiB write) between steps.
+  e2e    the reference-facing driver call mcq_run_qmc (run_qmc_cuda's entry point) at
+         eps = 1e-3 from 2^14 points per replica, doubling until var_of_means < eps^2/2, with
+         host structs in and the result read back; path-steps of the whole adaptive run over
+         host wall time.
+Multi-GPU (torchrun): every rank prices its own 32 replicas (salts offset by rank), no
+collective on the data path; max over ranks of the device time; "scaling": "weak".
+--impl reference times the reference algorithm's CPU restatement (the oracle) on the host
+cores on a bounded sample of the same workload (the reference has no CPU path of its own).
+"""
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "financial-derivatives-montecarlo_b200")
+
+S0, K, R_, SIG, T_, STEPS, REPS, SALT = 100.0, 100.0, 0.03, 0.25, 1.0, 256, 32, 42
+METRIC = "path-steps/s"
+# Algorithmic FP32 work per path-step of the raw Sobol GBM Asian path (counted as written,
+# FMA = 2 flops): u from the scrambled integer (I2F, add, mul: 2 flops), the inverse normal as
+# one AS241 central-region rational (7 + 7 FMA + 1 div: 29 flops), the GBM step
+# S (1 + mu h + sigma sqrt(h) z) (2 FMA: 4 flops), the Kahan-compensated running sum (4 flops).
+FLOPS_PER_PATH_STEP = 2 + 29 + 4 + 4
+
+
+def load_engine():
+    spec = importlib.util.spec_from_file_location("fdmc_b200", os.path.join(PKG, "__init__.py"),
+                                                  submodule_search_locations=[PKG])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["fdmc_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_baseline(seconds=12.0, steps=1):
+    """Oracle (CPU restatement, FP64 paths) on all host threads: returns path-steps/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as orc
+    T = orc.T
+    m, p = T.gbm(S0, R_, SIG, T_), T.asian(K)
+    threads = orc.max_threads()
+    # size the sample to about `seconds` of wall time from a short calibration run
+    n = 256
+    t0 = time.perf_counter()
+    orc.qmc_sums(m, p, STEPS, None, SALT, REPS, 0, n, 0, threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    n = max(256, int(n * seconds / dt) // 256 * 256)
+    vals = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        orc.qmc_sums(m, p, STEPS, None, SALT, REPS, 0, n, 0, threads)
+        dt = time.perf_counter() - t0
+        vals.append(REPS * n * STEPS / dt)
+    v = sorted(vals)[len(vals) // 2]
+    return {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{REPS} replicas x {n} points x {STEPS} steps of the same workload (FP64 oracle)"}
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    steps = []
+    cb = None
+    per = max(2.0, 60.0 / max(args.steps + args.warmup, 1))
+    for i in range(args.warmup + args.steps):
+        c = cpu_baseline(seconds=per, steps=1)
+        if i >= args.warmup:
+            steps.append(c["value"])
+            cb = c
+    v = sorted(steps)[len(steps) // 2]
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "RQMC arithmetic Asian call, GBM S0=K=100 r=0.03 sigma=0.25 T=1, "
+                                   "256 steps / Sobol dims, R=32 HH-scrambled replicas, raw ordering"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--points", type=int, default=1 << 18, help="points per replica per step")
+    ap.add_argument("--e2e-runs", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    eng = load_engine()
+    eng.init(local_rank)
+    m, p = eng.gbm(S0, R_, SIG, T_), eng.asian(K)
+    salt = SALT + REPS * rank
+    N = args.points
+    sums = torch.zeros(REPS * 2, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def one_pass():
+        eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, salt_base=salt, R=REPS, offset=0, n_points=N)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        one_pass()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            evs[i][0].record(stream)
+            one_pass()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ps_per_step = REPS * N * STEPS
+    value = world * ps_per_step * args.steps / (total_ms * 1e-3)
+    chk = sums.cpu().numpy().reshape(REPS, 2)
+    price = float((chk[:, 0] / N).mean())
+
+    # e2e: the reference-facing adaptive driver with host structs
+    cfg = eng.qmc_cfg(R=REPS, N0_per_replica=1 << 14, salt_base=salt)
+    eng.run_qmc(m, p, 1e-3, STEPS, cfg)   # warm-up (tables, streams)
+    e2e_ps, e2e_t, e2e_last = 0.0, 0.0, None
+    for _ in range(args.e2e_runs):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = eng.run_qmc(m, p, 1e-3, STEPS, cfg)
+        e2e_t += time.perf_counter() - t0
+        e2e_ps += r["path_steps"]
+        e2e_last = r
+    if world > 1:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_value = world * e2e_ps / e2e_t
+    doublings = max(1, int(round(__import__("math").log2(e2e_last["n_samples"] / (REPS << 14)))) + 1)
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peaks = measured_peaks()
+    clocks = clk.summary()
+    sm_count = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    mhz = clocks["sm_mhz"] or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or 1965.0
+    peak_fp32 = sm_count * 128 * 2 * mhz * 1e6 / 1e12
+    per_launch_ms = total_ms / args.steps
+    achieved = ps_per_step * FLOPS_PER_PATH_STEP / (per_launch_ms * 1e-3) / 1e12
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        traffic = tj["bytes_per_path_step"] * ps_per_step
+    except (OSError, ValueError, KeyError):
+        pass
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "RQMC arithmetic Asian call, GBM S0=K=100 r=0.03 sigma=0.25 T=1, 256 steps "
+                               "= 256 Sobol dims, R=32 HH-scrambled replicas, raw ordering",
+                   "points_per_replica_per_step": N, "replicas_per_gpu": REPS, "global_batch": world * REPS * N,
+                   "seq_len": STEPS, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "l2": "flushed (256 MiB write) between steps; inputs are parameter-sized"},
+        "price_check": price,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": doublings * REPS * 2 * 8,
+                "what": "mcq_run_qmc (run_qmc_cuda entry) eps=1e-3 from 2^14 pts/replica, host wall time; "
+                        "inputs are host parameter structs (kernel arguments), no array copies",
+                "price": e2e_last["price"], "std_error": e2e_last["std_error"], "n_samples": e2e_last["n_samples"],
+                "path_steps_per_run": e2e_last["path_steps"], "ms_per_run": 1e3 * e2e_t / args.e2e_runs},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                     "frac": achieved / peak_fp32, "traffic": traffic,
+                     "peak_source": f"derived: {sm_count} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock "
+                                    "sampled under load); MEASURED_PEAKS.json has no FP32 figure",
+                     "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel": "k_pass<Sobol, raw, PathC<GBM, Asian>>"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,30 @@
+// dispatch.h — lookup of the fused pass kernel instantiated for a (generator, noise, estimator,
+// model, payoff) combination.  The instantiations are spread over several translation units
+// so that they compile in parallel; each returns nullptr for a combination it does not hold.
+#pragma once
+#include "kparams.h"
+
+namespace mcq {
+
+const void* lookup_sobol_raw_plain(int model, int payoff);
+const void* lookup_sobol_raw_coupled(int model, int payoff);
+const void* lookup_sobol_bb(int model, int payoff, bool coupled);
+const void* lookup_philox_plain(int model, int payoff);
+const void* lookup_philox_coupled(int model, int payoff);
+// est in {EST_CV_ASIAN, EST_CV_DUPIRE, EST_IS}, basket models (nb = 4, 8, 16), dump probes
+const void* lookup_misc(int gen, int noise, int est, int model, int nb, bool dump);
+
+inline const void* lookup_pass(int gen, int noise, int est, int model, int payoff, int nb) {
+    if (model == MOD_MULTI || model == MOD_BASKET || est >= EST_CV_ASIAN)
+        return lookup_misc(gen, noise, est, model, nb, false);
+    const bool cpl = (est == EST_COUPLED);
+    if (gen == GEN_SOBOL) {
+        if (noise == NOISE_RAW) return cpl ? lookup_sobol_raw_coupled(model, payoff) : lookup_sobol_raw_plain(model, payoff);
+        if (noise == NOISE_BB) return lookup_sobol_bb(model, payoff, cpl);
+        return nullptr;
+    }
+    if (noise != NOISE_RAW) return nullptr;
+    return cpl ? lookup_philox_coupled(model, payoff) : lookup_philox_plain(model, payoff);
+}
+
+}  // namespace mcq

@@ -1,0 +1,391 @@
+// engine.cpp — device context, workspaces, parameter translation and the pass launcher.
+#include "engine.h"
+
+#include <curand.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "dispatch.h"
+#include "support.h"
+
+namespace mcq {
+
+// ------------------------------------------------------------------ buffers
+
+void* DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return p;
+    release();
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        throw Error(MCQ_ERR_NOMEM, "device allocation of " + std::to_string(want) + " bytes failed");
+    }
+    cap = want;
+    return p;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+void* PinnedBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return p;
+    release();
+    size_t want = std::max<size_t>(bytes, 256);
+    if (cudaMallocHost(&p, want) != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        throw Error(MCQ_ERR_NOMEM, "pinned allocation failed");
+    }
+    cap = want;
+    return p;
+}
+void PinnedBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+}
+
+void Workspace::ensure_stream() {
+    if (!stream) MCQ_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+}
+Workspace::~Workspace() {
+    if (stream) cudaStreamDestroy(stream);
+}
+
+// ------------------------------------------------------------------ engine
+
+Engine& engine() {
+    static Engine e;
+    return e;
+}
+
+Workspace& Engine::ws(int i) {
+    while ((int)pool.size() <= i) pool.emplace_back(new Workspace());
+    pool[i]->ensure_stream();
+    return *pool[i];
+}
+
+void ensure_ready(int device) {
+    Engine& E = engine();
+    if (E.ready && (device < 0 || device == E.device)) return;
+    if (E.ready) shutdown_engine();
+    int dev = device;
+    if (dev < 0) MCQ_CUDA(cudaGetDevice(&dev));
+    MCQ_CUDA(cudaSetDevice(dev));
+    cudaDeviceProp prop;
+    MCQ_CUDA(cudaGetDeviceProperties(&prop, dev));
+    MCQ_REQUIRE(prop.major >= 10, MCQ_ERR_UNSUPPORTED,
+                "this engine is built for sm_100a (B200); device " + std::string(prop.name) +
+                    " is sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
+    E.device = dev;
+    E.sm_count = prop.multiProcessorCount;
+    // JoeKuo6 direction vectors, as ensure_sobol_dirvectors_uploaded (methods_cuda.cu:764-775).
+    curandDirectionVectors32_t* hv = nullptr;
+    MCQ_REQUIRE(curandGetDirectionVectors32(&hv, CURAND_DIRECTION_VECTORS_32_JOEKUO6) ==
+                    CURAND_STATUS_SUCCESS,
+                MCQ_ERR_INTERNAL, "curandGetDirectionVectors32 failed");
+    MCQ_CUDA(cudaMalloc(&E.d_dv, sizeof(uint32_t) * 20000 * 32));
+    MCQ_CUDA(cudaMemcpy(E.d_dv, hv, sizeof(uint32_t) * 20000 * 32, cudaMemcpyHostToDevice));
+    E.ready = true;
+}
+
+void shutdown_engine() {
+    Engine& E = engine();
+    if (!E.ready) return;
+    cudaDeviceSynchronize();
+    E.pool.clear();
+    E.kinfo.clear();
+    if (E.d_dv) cudaFree(E.d_dv);
+    E.d_dv = nullptr;
+    E.ready = false;
+}
+
+long long gpu_free_bytes_80() {   // gpu_free_bytes, methods_cuda.cu:258-263
+    size_t f = 0, t = 0;
+    MCQ_CUDA(cudaMemGetInfo(&f, &t));
+    return (long long)((double)f * 0.8);
+}
+
+// ------------------------------------------------------------------ parameter translation
+
+int noise_dim(const mcq_model& m) {   // model_noise_dim, models.hpp:78-87
+    switch (m.kind) {
+        case MCQ_MODEL_HESTON: return 2;
+        case MCQ_MODEL_MULTI_DUPIRE:
+        case MCQ_MODEL_BASKET_GBM: return m.n_assets;
+        default: return 1;
+    }
+}
+
+int nstat_of(int est) {
+    switch (est) {
+        case EST_COUPLED: return 4;
+        case EST_CV_ASIAN:
+        case EST_CV_DUPIRE: return 7;
+        default: return 2;
+    }
+}
+
+static int model_code(int kind) {
+    switch (kind) {
+        case MCQ_MODEL_GBM: return MOD_GBM;
+        case MCQ_MODEL_HESTON: return MOD_HESTON;
+        case MCQ_MODEL_DUPIRE: return MOD_DUPIRE;
+        case MCQ_MODEL_MULTI_DUPIRE: return MOD_MULTI;
+        case MCQ_MODEL_LOCALVOL_GRID: return MOD_LVGRID;
+        case MCQ_MODEL_BASKET_GBM: return MOD_BASKET;
+    }
+    throw Error(MCQ_ERR_INVALID, "unknown model kind " + std::to_string(kind));
+}
+
+static bool is_pow2(long long x) { return x > 0 && (x & (x - 1)) == 0; }
+
+static bool uniform_axis(const double* a, int n, double* a0, double* inv_d) {
+    if (!a || n < 2) return false;
+    double d = (a[n - 1] - a[0]) / (n - 1);
+    if (!(d > 0)) return false;
+    for (int i = 0; i < n; i++)
+        if (std::fabs(a[i] - (a[0] + d * i)) > 1e-9 * std::max(1.0, std::fabs(a[i]))) return false;
+    *a0 = a[0];
+    *inv_d = 1.0 / d;
+    return true;
+}
+
+// make_params (methods_cuda.cu:986-1053) in the engine's layout; aux arrays are staged in `ws`.
+static void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
+    const mcq_model& m = *a.m;
+    const mcq_payoff& p = *a.p;
+    std::memset(&k, 0, sizeof(k));
+    k.gen = a.gen;
+    k.noise = a.noise;
+    k.model = model_code(m.kind);
+    k.payoff = p.kind;
+    k.est = a.est;
+    k.n_steps = a.n_steps;
+    k.d_noise = noise_dim(m);
+    k.D = a.n_steps * k.d_noise;
+    k.flags = a.flags;
+    k.nstat = nstat_of(a.est);
+
+    const float Tf = (float)m.T;
+    const float h = a.mlmc_h ? (float)(m.T / a.n_steps) : Tf / (float)a.n_steps;
+    k.T = Tf;
+    k.h = h;
+    k.sqrt_h = sqrtf(h);
+    k.S0 = (float)m.S0;
+    k.inv_S0 = 1.0f / k.S0;
+    k.mu = (float)m.mu;
+    k.sigma = (float)m.sigma;
+    k.kappa = (float)m.kappa;
+    k.theta = (float)m.theta;
+    k.xi = (float)m.xi;
+    k.v0 = (float)m.v0;
+    k.L10 = (float)m.hes_L10;
+    k.L11 = (float)m.hes_L11;
+    k.em_f = (float)std::exp((double)(-k.kappa * h));
+    k.sigma0 = (float)m.sigma0;
+    k.alpha = (float)m.alpha;
+    k.bm1 = (float)m.beta_d - 1.0f;
+    if (m.kind == MCQ_MODEL_DUPIRE) k.sigma = k.sigma0;   // :1041 sigma_eff for the GBM control
+
+    if (a.est == EST_COUPLED) {
+        k.M = a.M;
+        k.n_coarse = a.level0 ? 0 : a.n_steps / a.M;
+        k.hc = (float)(m.T / std::max(k.n_coarse, 1));
+        k.em_c = (float)std::exp((double)(-k.kappa * k.hc));
+        if (a.level0) k.M = INT_MAX;   // the coarse path never steps on level 0
+    }
+
+    k.K = (float)p.K;
+    k.B = (float)p.B;
+    switch (p.kind) {
+        case MCQ_PAYOFF_EUROPEAN:
+        case MCQ_PAYOFF_BARRIER_UP_OUT:
+        case MCQ_PAYOFF_BARRIER_DOWN_OUT:
+        case MCQ_PAYOFF_BASKET: k.disc = (float)std::exp(-p.r * p.T); break;
+        default: k.disc = 1.0f;
+    }
+    if (p.kind == MCQ_PAYOFF_LOOKBACK || p.kind == MCQ_PAYOFF_BARRIER_UP_OUT ||
+        p.kind == MCQ_PAYOFF_BARRIER_DOWN_OUT) {   // d_apply_bgk, :326-331
+        const float sb = (float)p.sigma;
+        k.corr_f = (float)std::exp((double)(-0.5826f * sb * sqrtf(h)));
+        k.corr_c = (float)std::exp((double)(-0.5826f * sb * sqrtf(k.hc > 0 ? k.hc : h)));
+    } else {
+        k.corr_f = k.corr_c = 1.0f;
+    }
+    k.u_cap = (a.flags & MCQ_FLAG_COMPAT_U_INF) ? 1.0f : 0x1.fffffep-1f;
+    k.beta_cv = a.beta_cv;
+    k.E_ctrl = a.E_ctrl;
+    k.z_star = a.z_star;
+    k.ctrl_sigma = k.sigma0;
+    k.seed = a.seed;
+    k.stream_base = a.stream0;
+
+    // multi-asset parameters
+    if (m.kind == MCQ_MODEL_MULTI_DUPIRE || m.kind == MCQ_MODEL_BASKET_GBM) {
+        const int n = m.n_assets;
+        MCQ_REQUIRE(n >= 1, MCQ_ERR_INVALID, "basket needs n_assets >= 1");
+        MCQ_REQUIRE(n <= kMaxBasket, MCQ_ERR_UNSUPPORTED,
+                    "basket width " + std::to_string(n) + " exceeds the register-resident limit 16");
+        MCQ_REQUIRE(m.S0_vec != nullptr, MCQ_ERR_INVALID, "basket needs S0_vec");
+        if (m.kind == MCQ_MODEL_BASKET_GBM)
+            MCQ_REQUIRE(m.sigma_vec != nullptr, MCQ_ERR_INVALID, "basket needs sigma_vec");
+        std::vector<float> pk((size_t)3 * n + (size_t)n * n, 0.f);
+        for (int i = 0; i < n; i++) {
+            pk[i] = (float)m.S0_vec[i];
+            pk[n + i] = m.sigma_vec ? (float)m.sigma_vec[i] : 0.f;
+            pk[2 * n + i] = m.weights ? (float)m.weights[i] : 1.0f / n;
+        }
+        const bool unc = m.uncorrelated || !m.L;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++)
+                pk[3 * n + i * n + j] = unc ? (i == j ? 1.f : 0.f) : (float)m.L[i * n + j];
+        k.n_assets = n;
+        k.uncorrelated = unc ? 1 : 0;
+        k.inv_S0 = 1.0f / (float)m.S0_vec[0];     // c_p.S0 = S0[0] (:1046)
+        k.S0 = (float)m.S0_vec[0];
+        float* d = (float*)ws.aux.ensure(pk.size() * sizeof(float));
+        MCQ_CUDA(cudaMemcpyAsync(d, pk.data(), pk.size() * sizeof(float), cudaMemcpyHostToDevice, ws.stream));
+        k.bsk = d;
+    }
+    if (m.kind == MCQ_MODEL_LOCALVOL_GRID) {
+        double K0, iK, t0, it;
+        MCQ_REQUIRE(uniform_axis(m.lv_K, m.lv_nK, &K0, &iK) && uniform_axis(m.lv_t, m.lv_nt, &t0, &it),
+                    MCQ_ERR_UNSUPPORTED, "local-vol grid axes must be uniform with >= 2 nodes");
+        MCQ_REQUIRE(m.lv_sigma != nullptr, MCQ_ERR_INVALID, "local-vol grid needs lv_sigma");
+        const size_t nn = (size_t)m.lv_nK * m.lv_nt;
+        std::vector<float> g(nn);
+        for (size_t i = 0; i < nn; i++) g[i] = (float)m.lv_sigma[i];
+        float* d = (float*)ws.aux.ensure(nn * sizeof(float));
+        MCQ_CUDA(cudaMemcpyAsync(d, g.data(), nn * sizeof(float), cudaMemcpyHostToDevice, ws.stream));
+        k.lv = d;
+        k.lv_nK = m.lv_nK;
+        k.lv_nt = m.lv_nt;
+        k.lv_K0 = (float)K0;
+        k.lv_inv_dK = (float)iK;
+        k.lv_t0 = (float)t0;
+        k.lv_inv_dt = (float)it;
+    }
+}
+
+// ------------------------------------------------------------------ launcher
+
+static constexpr long long kTargetItems = 148LL * 16 * 6;   // fixed -> device-independent split
+
+static KernelInfo& kernel_info(const void* fn, size_t smem) {
+    Engine& E = engine();
+    auto it = E.kinfo.find(fn);
+    if (it != E.kinfo.end() && it->second.smem == smem) return it->second;
+    KernelInfo ki;
+    ki.smem = smem;
+    MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ki.blocks_per_sm, fn, kThreads, smem));
+    MCQ_REQUIRE(ki.blocks_per_sm > 0, MCQ_ERR_INTERNAL, "kernel does not fit on an SM");
+    E.kinfo[fn] = ki;
+    return E.kinfo[fn];
+}
+
+void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
+    Engine& E = engine();
+    MCQ_REQUIRE(a.m && a.p, MCQ_ERR_INVALID, "null model or payoff");
+    MCQ_REQUIRE(a.n_steps >= 1, MCQ_ERR_INVALID, "n_steps must be >= 1");
+    MCQ_REQUIRE(a.R >= 1, MCQ_ERR_INVALID, "R must be >= 1");
+    MCQ_REQUIRE(a.m->T > 0, MCQ_ERR_INVALID, "T must be > 0");
+    if (a.n_points == 0) {
+        MCQ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * a.R * nstat_of(a.est), ws.stream));
+        return;
+    }
+    KParams k;
+    fill_params(ws, a, k);
+    const int D = k.D;
+    int nb = 0;
+    if (k.model == MOD_MULTI || k.model == MOD_BASKET) nb = k.n_assets;
+
+    if (a.gen == GEN_SOBOL) {
+        MCQ_REQUIRE(D <= 20000, MCQ_ERR_RANGE,
+                    "Sobol dimension " + std::to_string(D) + " exceeds the direction table (20000)");
+        MCQ_REQUIRE(a.offset + a.n_points <= (1ull << 32), MCQ_ERR_RANGE,
+                    "Sobol point index beyond 2^32 (offset " + std::to_string(a.offset) + " + " +
+                        std::to_string(a.n_points) + ")");
+    }
+    if (a.noise == NOISE_BB) {
+        MCQ_REQUIRE(k.d_noise == 1, MCQ_ERR_UNSUPPORTED, "Brownian bridge needs a one-factor model");
+        MCQ_REQUIRE(a.bb && a.bb->kind == MCQ_NOISE_BB && a.bb->n == a.n_steps, MCQ_ERR_INVALID,
+                    "Brownian-bridge handle missing or built for a different step count");
+        MCQ_REQUIRE(a.gen == GEN_SOBOL, MCQ_ERR_UNSUPPORTED, "Brownian bridge is a QMC transform");
+        k.bb = (const float4*)a.bb->table.p;
+        k.bbi = (const int2*)((const float4*)a.bb->table.p + a.n_steps);
+    }
+    MCQ_REQUIRE(a.noise != NOISE_PCA, MCQ_ERR_UNSUPPORTED, "PCA pass not available in this build");
+
+    const void* fn = a.dump ? lookup_misc(a.gen, a.noise, a.est, k.model, nb, true)
+                            : lookup_pass(a.gen, a.noise, a.est, k.model, a.p->kind, nb);
+    MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED,
+                "no fused kernel for gen " + std::to_string(a.gen) + " noise " + std::to_string(a.noise) +
+                    " est " + std::to_string(a.est) + " model " + std::to_string(a.m->kind) + " payoff " +
+                    std::to_string(a.p->kind));
+
+    // work split: 32-point groups, `gpi` groups per item, items per replica
+    const uint64_t g0 = a.offset >> 5;
+    const uint64_t G = ((a.offset + a.n_points - 1) >> 5) - g0 + 1;
+    uint64_t gpi = (G * (uint64_t)a.R + kTargetItems - 1) / kTargetItems;
+    if (gpi < 1) gpi = 1;
+    const uint64_t ipr = (G + gpi - 1) / gpi;
+    MCQ_REQUIRE(ipr * (uint64_t)a.R < (1ull << 31), MCQ_ERR_RANGE, "too many work items");
+    k.R = a.R;
+    k.gpi = (int)gpi;
+    k.items_per_rep = (int)ipr;
+    k.n_items = (int)(ipr * a.R);
+    k.offset = a.offset;
+    k.n_points = a.n_points;
+    k.g0 = g0;
+    k.G = G;
+
+    if (a.gen == GEN_SOBOL) {
+        if (!(ws.dirs_salt0 == a.salt0 && ws.dirs_R == a.R && ws.dirs_D == D)) {
+            uint32_t* d = (uint32_t*)ws.dirs.ensure(sizeof(uint32_t) * (size_t)a.R * 33 * D);
+            launch_prescramble(E.d_dv, a.salt0, a.R, D, d, ws.stream);
+            E.launches++;
+            ws.dirs_salt0 = a.salt0;
+            ws.dirs_R = a.R;
+            ws.dirs_D = D;
+        }
+        k.dirs = (const uint32_t*)ws.dirs.p;
+    }
+    const int nst = a.dump ? 1 : k.nstat;
+    k.nstat = nst;
+    k.partials = (double*)ws.partials.ensure(sizeof(double) * (size_t)k.n_items * nst);
+    if (a.dump) {
+        k.dump = (float*)ws.dump.ensure(sizeof(float) * (size_t)a.R * a.n_points * D);
+    }
+
+    const int skel = (a.noise == NOISE_BB && D > 32) ? ((D >> 5) + 1) * 32 : 0;
+    const size_t smem = (size_t)kWarpsPerBlock * (1024 + skel) * sizeof(float);
+    KernelInfo& ki = kernel_info(fn, smem);
+    long long blocks = ((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    blocks = std::min<long long>(blocks, (long long)ki.blocks_per_sm * E.sm_count);
+    blocks = std::max<long long>(blocks, 1);
+    void* args[] = {&k};
+    MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kThreads), args, smem, ws.stream));
+    launch_finalize(k.partials, a.R, k.items_per_rep, nst, d_out, ws.stream);
+    E.launches += 2;
+    MCQ_CUDA(cudaGetLastError());
+}
+
+std::vector<double> pass_sync(Workspace& ws, const PassArgs& a) {
+    const size_t n = (size_t)a.R * (a.dump ? 1 : nstat_of(a.est));
+    double* d = (double*)ws.sums.ensure(sizeof(double) * n);
+    pass_async(ws, a, d);
+    double* h = (double*)ws.hsums.ensure(sizeof(double) * n);
+    MCQ_CUDA(cudaMemcpyAsync(h, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ws.stream));
+    MCQ_CUDA(cudaStreamSynchronize(ws.stream));
+    return std::vector<double>(h, h + n);
+}
+
+}  // namespace mcq

@@ -1,0 +1,127 @@
+// engine.h — host runtime of the pricing engine: device context, per-stream workspaces,
+// BB/PCA handles, parameter translation and the fused-pass launcher.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/mcq.h"
+#include "kparams.h"
+
+namespace mcq {
+
+// Errors cross the C ABI as status codes; inside the library they are exceptions.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define MCQ_CUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            throw ::mcq::Error(MCQ_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e_) + \
+                                                 " at " __FILE__ ":" + std::to_string(__LINE__)); \
+    } while (0)
+
+#define MCQ_REQUIRE(cond, code, msg) \
+    do { if (!(cond)) throw ::mcq::Error((code), (msg)); } while (0)
+
+// Grow-only device / pinned-host buffers.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void* ensure(size_t bytes);
+    void release();
+    ~DevBuf() { release(); }
+};
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void* ensure(size_t bytes);
+    void release();
+    ~PinnedBuf() { release(); }
+};
+
+// Scratch owned by one stream: item partials, per-replica sums, scrambled direction words,
+// small parameter uploads.  Launches on one workspace are ordered by its stream.
+struct Workspace {
+    cudaStream_t stream = nullptr;
+    DevBuf partials, sums, dirs, aux, dump;
+    PinnedBuf hsums, haux;
+    uint32_t dirs_salt0 = 0;
+    int dirs_R = -1, dirs_D = -1;
+    void ensure_stream();
+    ~Workspace();
+};
+
+// BB / PCA handle (DeviceBBData / DevicePCAData, methods_cuda.cu:912-926).
+struct Handle {
+    int kind = 0;       // MCQ_NOISE_BB or MCQ_NOISE_PCA
+    int n = 0;
+    double T = 0;
+    DevBuf table;       // BB: float4[N] + int2[N]; PCA: fp16 [m][m] row-major (row = output step)
+    std::vector<float> host_f;   // BB: wl,wr,sd per dim; PCA: column-major float M
+    std::vector<int> host_i;     // BB: m per dim
+};
+
+struct KernelInfo {
+    int blocks_per_sm = 0;
+    size_t smem = 0;
+};
+
+struct Engine {
+    std::mutex mu;
+    bool ready = false;
+    int device = -1;
+    int sm_count = 148;
+    uint32_t* d_dv = nullptr;                        // JoeKuo6 table [20000][32]
+    std::vector<std::unique_ptr<Workspace>> pool;    // pool[0] is the default workspace
+    std::unordered_map<const void*, KernelInfo> kinfo;
+    int launches = 0;                                // kernel launches issued (accounting)
+    Workspace& ws(int i);
+};
+
+Engine& engine();
+void ensure_ready(int device = -1);
+void shutdown_engine();
+
+// Everything a fused pass needs besides the geometry of the work.
+struct PassArgs {
+    const mcq_model* m = nullptr;
+    const mcq_payoff* p = nullptr;
+    int n_steps = 0;          // fine steps
+    int est = EST_PLAIN;
+    int M = 0;                // coupling factor (EST_COUPLED)
+    bool level0 = false;      // coupled pass without a coarse path
+    bool mlmc_h = false;      // h = (float)(T / n) as run_mlmc_cuda (else (float)T / n)
+    int gen = GEN_SOBOL;
+    int noise = NOISE_RAW;
+    const Handle* bb = nullptr;
+    const Handle* pca = nullptr;
+    uint32_t salt0 = 42;
+    int R = 1;
+    uint64_t offset = 0;
+    uint64_t n_points = 0;
+    uint32_t seed = 0;
+    uint32_t stream0 = 0;
+    int flags = 0;
+    float beta_cv = 0.f, E_ctrl = 0.f, z_star = 0.f;
+    bool dump = false;
+};
+
+int noise_dim(const mcq_model& m);
+int nstat_of(int est);
+// Enqueue one pass on ws.stream; d_out receives [R][nstat] doubles (device).
+void pass_async(Workspace& ws, const PassArgs& a, double* d_out);
+// Enqueue, copy back and wait; returns [R][nstat].
+std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
+// Device capacity used by the reference's memory-derived batch sizing.
+long long gpu_free_bytes_80();
+
+}  // namespace mcq

@@ -1,0 +1,82 @@
+// kparams.h — parameter block shared by the host launch code and the device kernels.
+//
+// One KParams value describes one fused kernel pass: which generator, noise transform, model
+// and payoff, the path geometry, the work split into warp items, and where the per-item
+// partial sums go.  It replaces the reference's `__constant__ KernelParams c_p`
+// (methods_cuda.cu:211-246): it travels by value as a __grid_constant__ kernel argument, so
+// passes with different parameters can be in flight on different streams at the same time
+// (the reference has to keep c_p level-independent for exactly that reason, :1322-1324).
+#pragma once
+#include <cstdint>
+#include <vector_types.h>
+
+namespace mcq {
+
+enum Gen : int { GEN_SOBOL = 0, GEN_PHILOX = 1 };
+enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2 };
+enum ModelK : int { MOD_GBM = 0, MOD_HESTON = 1, MOD_DUPIRE = 2, MOD_MULTI = 3, MOD_LVGRID = 4, MOD_BASKET = 5 };
+enum PayK : int { PAY_EUR = 0, PAY_ASIAN = 1, PAY_GEOM = 2, PAY_LOOKBACK = 3, PAY_UPOUT = 4, PAY_BASKET = 5, PAY_DOWNOUT = 6 };
+enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE = 3, EST_IS = 4 };
+
+constexpr int kWarpsPerBlock = 8;
+constexpr int kThreads = kWarpsPerBlock * 32;
+constexpr int kMaxBasket = 16;          // register-resident basket width
+constexpr int kMaxStats = 8;
+
+struct KParams {
+    // ---- geometry
+    int gen, noise, model, payoff, est;
+    int n_steps;        // fine steps
+    int d_noise;        // normals per step
+    int D;              // n_steps * d_noise (Sobol dimensions / normals per path)
+    int M;              // coupling factor (EST_COUPLED); coarse step every M fine steps
+    int n_coarse;       // 0 on level 0 (no coarse path)
+    int flags;
+    int nstat;
+    // ---- work split: R replicas x [offset, offset + n_points) points in 32-point groups
+    int R;
+    int gpi;            // groups per item
+    int items_per_rep;
+    int n_items;
+    uint64_t offset;    // first point (Sobol index / Philox path id)
+    uint64_t n_points;  // points per replica
+    uint64_t g0;        // first group = offset >> 5
+    uint64_t G;         // groups per replica
+    // ---- model (single precision, as the reference's c_p)
+    float S0, inv_S0, mu, T, h, sqrt_h, sigma;
+    float kappa, theta, xi, L10, L11, v0, em_f;    // em_f = exp(-kappa h)
+    float sigma0, alpha, bm1;                      // Dupire: bm1 = beta_d - 1
+    float hc, em_c;                                // coarse step, exp(-kappa hc)
+    // ---- payoff
+    float K, B, disc, corr_f, corr_c, u_cap;
+    // ---- control variate / importance sampling
+    float beta_cv, E_ctrl, z_star;
+    float ctrl_sigma;                              // GBM control volatility (EST_CV_DUPIRE)
+    // ---- basket: packed [S0 | sigma | weight | L(n x n row-major)], float
+    int n_assets;
+    int uncorrelated;
+    const float* bsk;
+    // ---- local-vol grid sigma[j * nK + i], uniform axes
+    const float* lv;
+    int lv_nK, lv_nt;
+    float lv_K0, lv_inv_dK, lv_t0, lv_inv_dt;
+    // ---- Brownian bridge, one row per Sobol dimension j (= bb_precompute step j):
+    //      bb[j] = {wl, wr, sd, bits(m)}, bbi[j] = {l, r}
+    const float4* bb;
+    const int2* bbi;
+    // ---- PCA: M_pca (fp16, K-major rows = output step) device pointer
+    const void* pca;
+    // ---- Sobol: pre-scrambled words, replica r at dirs + r * 33 * D, word k of dim d at
+    //      [k * D + d] (k = 32 is the digital shift)
+    const uint32_t* dirs;
+    // ---- Philox
+    uint32_t seed, stream_base;
+    // ---- output: per-item partial sums [n_items][nstat]
+    double* partials;
+    // ---- parity dump (DumpC only): [R][n_points][D] normals (raw) or increments (bridge)
+    float* dump;
+    // ---- bounded-wait / error reporting
+    int* err;
+};
+
+}  // namespace mcq

@@ -1,0 +1,645 @@
+// path_kernels.cuh — the fused path kernel for sm_100a.
+//
+// One launch prices R replicas x n_points paths end to end: point generation (scrambled
+// Sobol or Philox), noise transform (raw, Brownian bridge), Euler stepping of the model,
+// running payoff accumulator, payoff / control-variate / importance-sampling weights,
+// Kahan accumulation per lane and a warp-shuffle reduction per work item.  No path array
+// is ever written to HBM; the only global writes are one partial-sum record per item.
+//
+// This fuses what the reference does in up to five passes over a D x N array in HBM:
+//   kernel_gen_hh_scrambled_sobol_normal / curandGenerateNormal   (methods_cuda.cu:799-825)
+//   kernel_scale / kernel_bb_transform                             (:561-594, :714-718)
+//   kernel_mc / kernel_mlmc / kernel_gbm_asian_cv / kernel_dupire_gbm_cv / kernel_is_gbm
+//   with CUB_REDUCE2/4 + atomicAdd                                 (:359-381, :414-707)
+//
+// Work layout.  Points are taken in aligned groups of 32 consecutive indices, one group per
+// warp at a time (lane i owns point 32h + i).  A work item is a run of `gpi` groups of one
+// replica; warps take items round-robin.  Item boundaries depend only on the problem size, so
+// the result is bit-reproducible run to run.
+//
+// Sobol generation (warp-transposed).  For a tile of 32 dimensions, lane j owns dimension
+// d0 + j and produces its scrambled integers for all 32 points of the group by gray-code
+// recurrence: x(32h) = shift ^ XOR_{k in gray(h)} Lv[5+k] ^ [h odd] Lv[4], then
+// x(32h+i+1) = x(32h+i) ^ Lv[ctz(i+1)].  Lv are the direction words already multiplied by the
+// replica's Hong–Hickernell matrix (linearity of the scramble over F2), so each point costs
+// one XOR instead of 32 splitmix32 rows + 32 popcounts (hh_scramble, methods_cuda.cu:781-795).
+// The normals go through a 32x32 XOR-swizzled shared-memory transpose and come back one row
+// (one path) per lane.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <type_traits>
+#include "kparams.h"
+
+namespace mcq {
+
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kTwoPow32Inv = 2.3283064365386963e-10f;   // 2^-32
+constexpr float kTwoPow24Inv = 5.9604644775390625e-08f;   // 2^-24
+
+__host__ __device__ constexpr int cx_ctz(int v) { return (v & 1) ? 0 : 1 + cx_ctz(v >> 1); }
+
+// ------------------------------------------------------------------ hashing / scrambling
+
+// splitmix32 (methods_cuda.cu:753-759).
+__host__ __device__ __forceinline__ uint32_t splitmix32(uint32_t x) {
+    x += 0x9E3779B9u;
+    x = (x ^ (x >> 16)) * 0x21F0AAADu;
+    x = (x ^ (x >> 15)) * 0x735A2D97u;
+    return x ^ (x >> 15);
+}
+
+// Hong–Hickernell lower-triangular F2 matrix applied to v, row k MSB-first, without the
+// digital shift (the linear part of hh_scramble, methods_cuda.cu:781-795).
+__device__ __forceinline__ uint32_t hh_linear(uint32_t v, uint32_t base) {
+    uint32_t out = 0;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        uint32_t seed = splitmix32(base ^ (uint32_t)k);
+        uint32_t mask = (k == 0) ? 0u : (0xFFFFFFFFu << (32 - k));
+        uint32_t row = (1u << (31 - k)) | (seed & mask);
+        out |= ((uint32_t)__popc(row & v) & 1u) << (31 - k);
+    }
+    return out;
+}
+
+// u = ((float)s + 1) * 2^-32 as in methods_cuda.cu:823; u_cap is 1.0f in reference-compat
+// mode (u may be 1 -> +inf) and 1 - 2^-24 otherwise.
+__device__ __forceinline__ float sobol_normal(uint32_t x, float u_cap) {
+    float u = ((float)x + 1.0f) * kTwoPow32Inv;
+    return normcdfinvf(fminf(u, u_cap));
+}
+
+// ------------------------------------------------------------------ transpose buffer
+
+// 32 x 32 floats per warp, 16-byte chunks XOR-swizzled by row so that column writes
+// (lane = column) and float4 row reads (lane = row) are both bank-conflict free.
+__device__ __forceinline__ int swz(int row, int col) {
+    return row * 32 + ((((col >> 2) ^ (row & 7)) << 2) | (col & 3));
+}
+
+__device__ __forceinline__ void read_row(const float* buf, int lane, float (&z)[32]) {
+    const float4* b4 = reinterpret_cast<const float4*>(buf + lane * 32);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        float4 v = b4[c ^ (lane & 7)];
+        z[4 * c + 0] = v.x; z[4 * c + 1] = v.y; z[4 * c + 2] = v.z; z[4 * c + 3] = v.w;
+    }
+}
+
+// Lane owns dimension `dim` of replica table `dr` (words [k * D + dim]); writes the normals of
+// points 32h .. 32h+31 into column `lane` of the transpose buffer.
+__device__ __forceinline__ void sobol_tile(const uint32_t* __restrict__ dr, int D, int dim,
+                                           bool active, uint64_t h, float u_cap, float* buf,
+                                           int lane) {
+    if (!active) return;
+    const uint32_t* col = dr + dim;
+    const uint32_t L0 = __ldg(col), L1 = __ldg(col + D), L2 = __ldg(col + 2 * D),
+                   L3 = __ldg(col + 3 * D), L4 = __ldg(col + 4 * D);
+    uint32_t x = __ldg(col + 32 * D);
+    if (h & 1) x ^= L4;
+    uint32_t g = (uint32_t)(h ^ (h >> 1));
+    while (g) {
+        const int k = __ffs(g) - 1;
+        x ^= __ldg(col + (5 + k) * D);
+        g &= g - 1;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+        buf[swz(i, lane)] = sobol_normal(x, u_cap);
+        if (i < 31) {
+            const int c = cx_ctz(i + 1);
+            x ^= (c == 0) ? L0 : (c == 1) ? L1 : (c == 2) ? L2 : (c == 3) ? L3 : L4;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ Philox4x32-10
+
+__device__ __forceinline__ uint4 philox10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r) { k.x += 0x9E3779B9u; k.y += 0xBB67AE85u; }
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    }
+    return c;
+}
+
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
+    const float u1 = ((float)(a >> 8) + 0.5f) * kTwoPow24Inv;
+    const float u2 = ((float)(b >> 8) + 0.5f) * kTwoPow24Inv;
+    const float rr = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    z0 = rr * s;
+    z1 = rr * c;
+}
+
+// Normals 32t .. 32t+31 of path `path` on stream `stream` (block b = dims 4b..4b+3).
+__device__ __forceinline__ void philox_tile(uint32_t seed, uint32_t stream, uint64_t path, int t,
+                                            float (&z)[32]) {
+    const uint2 key = make_uint2(seed, 0x6D637121u);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const uint4 o = philox10(make_uint4((uint32_t)(8 * t + q), (uint32_t)path,
+                                            (uint32_t)(path >> 32), stream), key);
+        box_muller(o.x, o.y, z[4 * q], z[4 * q + 1]);
+        box_muller(o.z, o.w, z[4 * q + 2], z[4 * q + 3]);
+    }
+}
+
+// ------------------------------------------------------------------ accumulation
+
+__device__ __forceinline__ void kadd(float& s, float& c, float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+template <int NST>
+struct Acc {
+    float s[NST], c[NST];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < NST; i++) s[i] = c[i] = 0.f;
+    }
+    __device__ __forceinline__ void add(const float (&y)[NST]) {
+#pragma unroll
+        for (int i = 0; i < NST; i++) kadd(s[i], c[i], y[i]);
+    }
+    // Warp total in FP64 (fixed shuffle order), lane 0 stores the item record.
+    __device__ __forceinline__ void flush(double* out, int lane) {
+#pragma unroll
+        for (int i = 0; i < NST; i++) {
+            double v = (double)s[i] - (double)c[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) out[i] = v;
+        }
+    }
+};
+
+// ------------------------------------------------------------------ models and payoffs
+
+__device__ __forceinline__ float lv_sigma(const KParams& p, float S, float t) {
+    float x = (S - p.lv_K0) * p.lv_inv_dK;
+    x = fminf(fmaxf(x, 0.f), (float)(p.lv_nK - 1));
+    const int i = min((int)x, p.lv_nK - 2);
+    const float a = x - (float)i;
+    float y = (t - p.lv_t0) * p.lv_inv_dt;
+    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
+    const int j = min((int)y, p.lv_nt - 2);
+    const float b = y - (float)j;
+    const float* g = p.lv + j * p.lv_nK + i;
+    const float s00 = __ldg(g), s01 = __ldg(g + 1), s10 = __ldg(g + p.lv_nK),
+                s11 = __ldg(g + p.lv_nK + 1);
+    const float lo = fmaf(a, s01 - s00, s00), hi = fmaf(a, s11 - s10, s10);
+    return fmaf(b, hi - lo, lo);
+}
+
+template <int PAY>
+__host__ __device__ constexpr bool path_dep() {
+    return PAY == PAY_ASIAN || PAY == PAY_GEOM || PAY == PAY_LOOKBACK || PAY == PAY_UPOUT ||
+           PAY == PAY_DOWNOUT;
+}
+
+// One discretisation of one single-asset path (d_euler_gbm / d_euler_heston / d_euler_dupire
+// and d_running_* / d_apply_bgk / d_payoff, methods_cuda.cu:270-352).  The Euler updates are
+// written as S * (1 + mu h + vol dW); the reference's S + mu S h + vol S dW differs only in
+// rounding.
+template <int MOD, int PAY>
+struct Leg {
+    float S, V, r0, r1;
+    __device__ __forceinline__ void init(const KParams& p) {
+        S = p.S0; V = p.v0; r1 = 0.f;
+        r0 = (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) ? p.S0 : 0.f;
+    }
+    __device__ __forceinline__ void update() {
+        if constexpr (PAY == PAY_ASIAN) kadd(r0, r1, S);
+        else if constexpr (PAY == PAY_GEOM) kadd(r0, r1, logf(S));
+        else if constexpr (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) r0 = fminf(r0, S);
+        else if constexpr (PAY == PAY_UPOUT) r0 = fmaxf(r0, S);
+    }
+    template <bool RUN>
+    __device__ __forceinline__ void step(const KParams& p, float dw1, float dw2, float t,
+                                         float omh, float em) {
+        if constexpr (MOD == MOD_GBM) {
+            S = S * fmaf(p.sigma, dw1, omh);
+        } else if constexpr (MOD == MOD_DUPIRE) {
+            const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S * p.inv_S0), -p.alpha * t * kLog2e));
+            S = S * fmaf(sl, dw1, omh);
+        } else if constexpr (MOD == MOD_LVGRID) {
+            const float sl = lv_sigma(p, S, t);
+            S = S * fmaf(sl, dw1, omh);
+        } else if constexpr (MOD == MOD_HESTON) {
+            const float sq = sqrtf(fmaxf(V, 0.f));
+            S = S * fmaf(sq, dw1, omh);
+            V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
+        }
+        if constexpr (RUN && path_dep<PAY>()) update();
+    }
+    __device__ __forceinline__ float payoff(const KParams& p, int n, float corr) const {
+        if constexpr (PAY == PAY_EUR || PAY == PAY_BASKET) return fmaxf(S - p.K, 0.f) * p.disc;
+        else if constexpr (PAY == PAY_ASIAN) return fmaxf((r0 - r1) / (float)n - p.K, 0.f);
+        else if constexpr (PAY == PAY_GEOM) return fmaxf(expf((r0 - r1) / (float)n) - p.K, 0.f);
+        else if constexpr (PAY == PAY_LOOKBACK) return S - r0 * corr;
+        else if constexpr (PAY == PAY_UPOUT) return (r0 / corr >= p.B) ? 0.f : fmaxf(S - p.K, 0.f) * p.disc;
+        else return (r0 * corr <= p.B) ? 0.f : fmaxf(S - p.K, 0.f) * p.disc;   // PAY_DOWNOUT
+    }
+};
+
+// ------------------------------------------------------------------ path consumers
+// A consumer takes the normals of its path in Sobol-dimension order (raw mode, tile by tile)
+// or the time-ordered increments (bridge mode) and produces the estimator's statistics.
+
+// Single-level / coupled fine-coarse path (kernel_mc, kernel_mlmc).
+template <int MOD, int PAY, bool COUPLED>
+struct PathC {
+    static constexpr int NST = COUPLED ? 4 : 2;
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    static constexpr bool HES = (MOD == MOD_HESTON);
+    Leg<MOD, PAY> f, c;
+    float a1, a2, omh_f, omh_c;
+    int k, m, ck;
+    bool run_upd;
+    __device__ __forceinline__ void init(const KParams& p) {
+        f.init(p);
+        omh_f = fmaf(p.mu, p.h, 1.0f);
+        k = 0;
+        run_upd = !(HES && COUPLED && (p.flags & 2));
+        if constexpr (COUPLED) { c.init(p); a1 = a2 = 0.f; m = 0; ck = 0; omh_c = fmaf(p.mu, p.hc, 1.0f); }
+    }
+    __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
+        const float t = (float)k * p.h;
+        if (run_upd) f.template step<true>(p, dw1, dw2, t, omh_f, p.em_f);
+        else f.template step<false>(p, dw1, dw2, t, omh_f, p.em_f);
+        k++;
+        if constexpr (COUPLED) {
+            a1 += dw1;
+            if constexpr (HES) a2 += dw2;
+            if (++m == p.M) {
+                const float tc = (float)ck * p.hc;
+                if (run_upd) c.template step<true>(p, a1, a2, tc, omh_c, p.em_c);
+                else c.template step<false>(p, a1, a2, tc, omh_c, p.em_c);
+                a1 = a2 = 0.f; m = 0; ck++;
+            }
+        }
+    }
+    // raw normals, tile of 32 dimensions starting at a tile boundary
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+        if constexpr (HES) {
+#pragma unroll
+            for (int i = 0; i < 16; i++)
+                if (2 * i < nv) {
+                    const float z1 = z[2 * i], z2 = z[2 * i + 1];
+                    step_dw(p, z1 * p.sqrt_h, fmaf(p.L10, z1, p.L11 * z2) * p.sqrt_h);
+                }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 32; i++)
+                if (i < nv) step_dw(p, z[i] * p.sqrt_h, 0.f);
+        }
+    }
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const float pf = f.payoff(p, p.n_steps, p.corr_f);
+        if constexpr (COUPLED) {
+            const float pc = (p.n_coarse > 0) ? c.payoff(p, p.n_coarse, p.corr_c) : 0.f;
+            const float dy = pf - pc;
+            y[0] = dy; y[1] = dy * dy; y[2] = pf; y[3] = pf * pf;
+        } else {
+            y[0] = pf; y[1] = pf * pf;
+        }
+    }
+};
+
+// Arithmetic Asian with geometric-Asian control on the same GBM path (kernel_gbm_asian_cv,
+// methods_cuda.cu:601-640): stats {Ya, Ya^2, Ycv, Ycv^2, Yg, Yg^2, Ya*Yg}.
+struct CvAsianC {
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    static constexpr int NST = 7;
+    float S, sa, ca, sl, cl, omh;
+    __device__ __forceinline__ void init(const KParams& p) {
+        S = p.S0; sa = ca = sl = cl = 0.f; omh = fmaf(p.mu, p.h, 1.0f);
+    }
+    __device__ __forceinline__ void step_dw(const KParams& p, float dw, float) {
+        S = S * fmaf(p.sigma, dw, omh);
+        kadd(sa, ca, S);
+        kadd(sl, cl, logf(S));
+    }
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv) step_dw(p, z[i] * p.sqrt_h, 0.f);
+    }
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const float n = (float)p.n_steps;
+        const float ya = fmaxf((sa - ca) / n - p.K, 0.f);
+        const float yg = fmaxf(expf((sl - cl) / n) - p.K, 0.f);
+        const float ycv = ya - p.beta_cv * (yg - p.E_ctrl);
+        y[0] = ya; y[1] = ya * ya; y[2] = ycv; y[3] = ycv * ycv;
+        y[4] = yg; y[5] = yg * yg; y[6] = ya * yg;
+    }
+};
+
+// Dupire European with a GBM European control on the same increments
+// (kernel_dupire_gbm_cv, methods_cuda.cu:642-677).
+struct CvDupireC {
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    static constexpr int NST = 7;
+    float Sd, Sg, omh;
+    int k;
+    __device__ __forceinline__ void init(const KParams& p) {
+        Sd = Sg = p.S0; omh = fmaf(p.mu, p.h, 1.0f); k = 0;
+    }
+    __device__ __forceinline__ void step_dw(const KParams& p, float dw, float) {
+        const float t = (float)k * p.h;
+        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(Sd * p.inv_S0), -p.alpha * t * kLog2e));
+        Sd = Sd * fmaf(sl, dw, omh);
+        Sg = Sg * fmaf(p.ctrl_sigma, dw, omh);
+        k++;
+    }
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv) step_dw(p, z[i] * p.sqrt_h, 0.f);
+    }
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const float yd = fmaxf(Sd - p.K, 0.f) * p.disc;
+        const float yg = fmaxf(Sg - p.K, 0.f) * p.disc;
+        const float ycv = yd - p.beta_cv * (yg - p.E_ctrl);
+        y[0] = yd; y[1] = yd * yd; y[2] = ycv; y[3] = ycv * ycv;
+        y[4] = yg; y[5] = yg * yg; y[6] = yd * yg;
+    }
+};
+
+// GBM European under the drift-shifted measure Z' = Z + z* with likelihood ratio
+// exp(-z* sum Z - N z*^2 / 2) (kernel_is_gbm, methods_cuda.cu:685-707).
+struct IsC {
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    static constexpr int NST = 2;
+    float S, zs, zc, omh;
+    __device__ __forceinline__ void init(const KParams& p) {
+        S = p.S0; zs = zc = 0.f; omh = fmaf(p.mu, p.h, 1.0f);
+    }
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv) {
+                kadd(zs, zc, z[i]);
+                S = S * fmaf(p.sigma, (z[i] + p.z_star) * p.sqrt_h, omh);
+            }
+    }
+    __device__ __forceinline__ void step_dw(const KParams&, float, float) {}
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const float lr = expf(-p.z_star * (zs - zc) - 0.5f * p.z_star * p.z_star * (float)p.n_steps);
+        const float v = fmaxf(S - p.K, 0.f) * p.disc * lr;
+        y[0] = v; y[1] = v * v;
+    }
+};
+
+// Multi-asset basket (kernel_multi_dupire, methods_cuda.cu:525-551, with the Cholesky product
+// of correlate_multi_dupire :1122-1148 done in registers): dims of step k are k*n + a.
+// MOD_MULTI: parametric Dupire per asset with the reference's asset-0 S0 inside sigma_loc
+// (:542, :289); MOD_BASKET: GBM per asset with its own sigma, weighted basket.
+template <int MOD, int NB>
+struct BasketC {
+    static constexpr int NST = 2;
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    float S[NB], dw[NB];
+    float omh;
+    int f, k;
+    __device__ __forceinline__ void init(const KParams& p) {
+        const int n = p.n_assets;
+#pragma unroll
+        for (int a = 0; a < NB; a++) { S[a] = (a < n) ? __ldg(p.bsk + a) : 0.f; dw[a] = 0.f; }
+        omh = fmaf(p.mu, p.h, 1.0f);
+        f = 0; k = 0;
+    }
+    __device__ __forceinline__ void feed(const KParams& p, float z) {
+        const int n = p.n_assets;
+        const float x = z * p.sqrt_h;
+        if (p.uncorrelated) {
+#pragma unroll
+            for (int a = 0; a < NB; a++) if (a == f) dw[a] = x;
+        } else {
+            const float* Lrow = p.bsk + 3 * n + f;   // L[a][f] at Lrow[a * n]
+#pragma unroll
+            for (int a = 0; a < NB; a++)
+                if (a >= f && a < n) dw[a] = fmaf(__ldg(Lrow + a * n), x, dw[a]);
+        }
+        if (++f == n) {
+            const float t = (float)k * p.h;
+#pragma unroll
+            for (int a = 0; a < NB; a++) {
+                if (a < n) {
+                    if constexpr (MOD == MOD_MULTI) {
+                        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * p.inv_S0), -p.alpha * t * kLog2e));
+                        S[a] = S[a] * fmaf(sl, dw[a], omh);
+                    } else {
+                        S[a] = S[a] * fmaf(__ldg(p.bsk + n + a), dw[a], omh);
+                    }
+                }
+                dw[a] = 0.f;
+            }
+            f = 0; k++;
+        }
+    }
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv) feed(p, z[i]);
+    }
+    __device__ __forceinline__ void step_dw(const KParams&, float, float) {}
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const int n = p.n_assets;
+        float b = 0.f;
+        if constexpr (MOD == MOD_MULTI) {
+#pragma unroll
+            for (int a = 0; a < NB; a++) if (a < n) b += S[a];
+            b = b / (float)n;
+        } else {
+#pragma unroll
+            for (int a = 0; a < NB; a++) if (a < n) b = fmaf(__ldg(p.bsk + 2 * n + a), S[a], b);
+        }
+        const float v = fmaxf(b - p.K, 0.f) * p.disc;
+        y[0] = v; y[1] = v * v;
+    }
+};
+
+// Parity probe: records the normals (raw) or increments (bridge) the pass consumed for one
+// path, so tests can compare the fused generation bit for bit with the reference stream.
+struct DumpC {
+    static constexpr int NST = 1;
+    float* out;
+    int idx;
+    bool on;
+    __device__ __forceinline__ void init(const KParams&) { idx = 0; }
+    __device__ __forceinline__ void bind(const KParams& p, int r, uint64_t n) {
+        on = n >= p.offset && n < p.offset + p.n_points;
+        out = p.dump + ((size_t)r * p.n_points + (size_t)(n - p.offset)) * (size_t)p.D;
+    }
+    __device__ __forceinline__ void tile(const KParams&, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv && on) out[idx + i] = z[i];
+        idx += nv;
+    }
+    __device__ __forceinline__ void step_dw(const KParams&, float dw, float) {
+        if (on) out[idx] = dw;
+        idx++;
+    }
+    __device__ __forceinline__ void finish(const KParams&, float (&y)[NST]) { y[0] = 0.f; }
+};
+
+// ------------------------------------------------------------------ Brownian bridge
+
+// Window of 32 increments from the bridge between W_L = W(32q) and W_R = W(32q + 32):
+// 31 interior points over five levels, all indices static.  zs[s] is the normal of interior
+// slot s (level u = floor(log2(s+1)), position v = s + 1 - 2^u); its Sobol dimension is
+// (S << u) + (q << u) + v (bb_precompute's level order, utils.cpp:78-99) and its weights are
+// read from the per-dimension table.
+template <class C>
+__device__ __forceinline__ void bb_window(const KParams& p, C& cons, const float (&zs)[32],
+                                          float WL, float WR, int S, int q) {
+    float W[33];
+    W[0] = WL;
+    W[32] = WR;
+#pragma unroll
+    for (int u = 0; u < 5; u++) {
+#pragma unroll
+        for (int v = 0; v < (1 << u); v++) {
+            const int s = (1 << u) - 1 + v;
+            const int half = 16 >> u;
+            const int mid = (2 * v + 1) * half, lft = 2 * v * half, rgt = (2 * v + 2) * half;
+            const int dim = (S << u) + (q << u) + v;
+            const float4 w = __ldg(p.bb + dim);
+            W[mid] = fmaf(w.x, W[lft], fmaf(w.y, W[rgt], w.z * zs[s]));
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 32; t++) cons.step_dw(p, W[t + 1] - W[t], 0.f);
+}
+
+// ------------------------------------------------------------------ the pass kernel
+
+template <int GEN, int NOISE, class C>
+__device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint32_t* dr,
+                                          uint32_t stream, uint64_t h, uint64_t n, float* buf,
+                                          float* skel, int lane) {
+    const int D = p.D;
+    if constexpr (NOISE == NOISE_RAW) {
+        for (int d0 = 0; d0 < D; d0 += 32) {
+            float z[32];
+            if constexpr (GEN == GEN_SOBOL) {
+                sobol_tile(dr, D, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
+                __syncwarp();
+                read_row(buf, lane, z);
+                __syncwarp();
+            } else {
+                philox_tile(p.seed, stream, n, d0 >> 5, z);
+            }
+            cons.tile(p, z, min(32, D - d0));
+        }
+    } else {   // NOISE_BB, one factor: D == n_steps == N (power of two)
+        // Bridge table row j (Sobol dimension j = bb_precompute step j, utils.cpp:54-101):
+        // p.bb[j] = {wl, wr, sd, bits(m)} and p.bbi[j] = {l, r}: W[m] = wl W[l] + wr W[r] + sd z_j.
+        const int N = D;
+        if (N <= 32) {
+            // one tile: the literal table-driven bridge (bb_apply, utils.cpp:104-124)
+            sobol_tile(dr, D, lane, lane < N, h, p.u_cap, buf, lane);
+            __syncwarp();
+            float z[32];
+            read_row(buf, lane, z);
+            __syncwarp();
+            float W[33];
+#pragma unroll
+            for (int i = 0; i < 33; i++) W[i] = 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                if (j < N) {
+                    const float4 w = __ldg(p.bb + j);
+                    const int2 lr = __ldg(p.bbi + j);
+                    W[__float_as_int(w.w)] = fmaf(w.x, W[lr.x], fmaf(w.y, W[lr.y], w.z * z[j]));
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 32; t++)
+                if (t < N) cons.step_dw(p, W[t + 1] - W[t], 0.f);
+        } else {
+            // Skeleton W(32q), q = 0..S, from dimensions 0..S-1 (all multiples of 32), kept
+            // per lane in shared memory at skel[q * 32 + lane]; then S windows of 32 steps.
+            const int S = N >> 5;
+            skel[lane] = 0.f;
+            for (int t0 = 0; t0 < S; t0 += 32) {
+                sobol_tile(dr, D, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const int dim = t0 + j;
+                    if (dim < S) {
+                        const float4 w = __ldg(p.bb + dim);
+                        const int2 lr = __ldg(p.bbi + dim);
+                        const int mi = __float_as_int(w.w) >> 5, li = lr.x >> 5, ri = lr.y >> 5;
+                        skel[mi * 32 + lane] = fmaf(w.x, skel[li * 32 + lane],
+                                                    fmaf(w.y, skel[ri * 32 + lane], w.z * z[j]));
+                    }
+                }
+            }
+            for (int q = 0; q < S; q++) {
+                int dim = 0;
+                const bool act = lane < 31;
+                if (act) {
+                    const int u = 31 - __clz(lane + 1);
+                    dim = (S << u) + (q << u) + (lane + 1 - (1 << u));
+                }
+                sobol_tile(dr, D, dim, act, h, p.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+                bb_window(p, cons, z, skel[q * 32 + lane], skel[(q + 1) * 32 + lane], S, q);
+            }
+        }
+    }
+}
+
+template <int GEN, int NOISE, class C>
+__global__ void __launch_bounds__(kThreads, 2) k_pass(const __grid_constant__ KParams p) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int skel_floats = (NOISE == NOISE_BB && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;
+    float* buf = reinterpret_cast<float*>(smem4) + wib * (1024 + skel_floats);
+    float* skel = buf + 1024;
+    const int total_warps = gridDim.x * kWarpsPerBlock;
+    const uint64_t gend_all = p.g0 + p.G;
+    for (int item = blockIdx.x * kWarpsPerBlock + wib; item < p.n_items; item += total_warps) {
+        const int r = item / p.items_per_rep;
+        const int j = item - r * p.items_per_rep;
+        const uint64_t gb = p.g0 + (uint64_t)j * (uint64_t)p.gpi;
+        const uint64_t ge = min(gb + (uint64_t)p.gpi, gend_all);
+        const uint32_t* dr = (GEN == GEN_SOBOL) ? p.dirs + (size_t)r * 33 * (size_t)p.D : nullptr;
+        const uint32_t stream = p.stream_base + (uint32_t)r;
+        Acc<C::NST> acc;
+        acc.zero();
+        for (uint64_t h = gb; h < ge; h++) {
+            const uint64_t n = h * 32 + (uint64_t)lane;
+            C cons;
+            cons.init(p);
+            if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
+            else cons.bind(r, n);
+            run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane);
+            float y[C::NST];
+            cons.finish(p, y);
+            if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
+        }
+        acc.flush(p.partials + (size_t)item * C::NST, lane);
+    }
+}
+
+}  // namespace mcq

@@ -1,0 +1,182 @@
+"""ctypes mirrors of the structs in include/mcq.h, plus builders for models and payoffs.
+
+This module only describes data; it loads no library.  The engine binding (this package's
+__init__) and the test oracle binding both use it.
+"""
+import ctypes as C
+
+import numpy as np
+
+# model / payoff / noise enumerations (include/mcq.h)
+GBM, HESTON, DUPIRE, MULTI_DUPIRE, LOCALVOL_GRID, BASKET_GBM = range(6)
+EUROPEAN, ASIAN, GEOM_ASIAN, LOOKBACK, BARRIER_UP_OUT, BASKET, BARRIER_DOWN_OUT = range(7)
+RAW, BB, PCA = range(3)
+FLAG_COMPAT_U_INF = 1
+FLAG_COMPAT_HESTON_MLMC = 2
+
+_pd = C.POINTER(C.c_double)
+
+
+class Model(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("n_assets", C.c_int32),
+        ("S0", C.c_double), ("mu", C.c_double), ("T", C.c_double),
+        ("sigma", C.c_double),
+        ("kappa", C.c_double), ("theta", C.c_double), ("xi", C.c_double), ("rho", C.c_double),
+        ("v0", C.c_double), ("hes_L10", C.c_double), ("hes_L11", C.c_double),
+        ("sigma0", C.c_double), ("alpha", C.c_double), ("beta_d", C.c_double),
+        ("uncorrelated", C.c_int32), ("_pad0", C.c_int32),
+        ("S0_vec", _pd), ("L", _pd), ("sigma_vec", _pd), ("weights", _pd),
+        ("lv_nK", C.c_int32), ("lv_nt", C.c_int32),
+        ("lv_K", _pd), ("lv_t", _pd), ("lv_sigma", _pd),
+    ]
+
+
+class Payoff(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_assets", C.c_int32), ("K", C.c_double), ("B", C.c_double),
+                ("r", C.c_double), ("T", C.c_double), ("sigma", C.c_double)]
+
+
+class MCCfg(C.Structure):
+    _fields_ = [("N_batch", C.c_int64), ("pilot_n", C.c_int32), ("seed", C.c_uint32)]
+
+
+class QMCCfg(C.Structure):
+    _fields_ = [("R", C.c_int32), ("max_doublings", C.c_int32), ("N0_per_replica", C.c_int64),
+                ("salt_base", C.c_uint32), ("flags", C.c_int32)]
+
+
+class MLMCCfg(C.Structure):
+    _fields_ = [("M", C.c_int32), ("max_L", C.c_int32), ("pilot_n", C.c_int32), ("n0_steps", C.c_int32),
+                ("flags", C.c_int32), ("seed", C.c_uint32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("price", C.c_double), ("std_error", C.c_double), ("n_samples", C.c_int64),
+                ("time_s", C.c_double), ("path_steps", C.c_double), ("levels", C.c_int32),
+                ("launches", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CVPilotOut(C.Structure):
+    _fields_ = [("beta", C.c_double), ("var_plain", C.c_double), ("var_cv", C.c_double)]
+
+
+def _arr(x):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+    return a, a.ctypes.data_as(_pd)
+
+
+def _keep(m, *arrays):
+    m._keep = getattr(m, "_keep", []) + list(arrays)
+    return m
+
+
+def gbm(S0=100.0, mu=0.05, sigma=0.2, T=1.0):
+    m = Model()
+    m.kind, m.S0, m.mu, m.sigma, m.T = GBM, S0, mu, sigma, T
+    return m
+
+
+def heston(S0=100.0, mu=0.05, kappa=2.0, theta=0.04, xi=0.5, rho=-0.9, v0=0.04, T=1.0):
+    m = Model()
+    m.kind, m.S0, m.mu, m.kappa, m.theta, m.xi, m.rho, m.v0, m.T = HESTON, S0, mu, kappa, theta, xi, rho, v0, T
+    m.hes_L10, m.hes_L11 = rho, float(np.sqrt(1.0 - rho * rho))
+    return m
+
+
+def dupire(S0=100.0, mu=0.05, sigma0=0.2, alpha=0.5, beta_d=0.7, T=1.0):
+    m = Model()
+    m.kind, m.S0, m.mu, m.sigma0, m.alpha, m.beta_d, m.T = DUPIRE, S0, mu, sigma0, alpha, beta_d, T
+    m.sigma = sigma0
+    return m
+
+
+def multi_dupire(S0_vec, L=None, mu=0.05, sigma0=0.2, alpha=0.5, beta_d=0.7, T=1.0):
+    m = Model()
+    s, ps = _arr(S0_vec)
+    m.kind, m.n_assets, m.mu, m.sigma0, m.alpha, m.beta_d, m.T = MULTI_DUPIRE, len(s), mu, sigma0, alpha, beta_d, T
+    m.S0, m.S0_vec = float(s[0]), ps
+    keep = [s]
+    if L is None:
+        m.uncorrelated = 1
+    else:
+        la, pl = _arr(L)
+        m.L = pl
+        keep.append(la)
+    return _keep(m, *keep)
+
+
+def basket_gbm(S0_vec, sigma_vec, L=None, weights=None, mu=0.05, T=1.0):
+    m = Model()
+    s, ps = _arr(S0_vec)
+    sg, psg = _arr(sigma_vec)
+    m.kind, m.n_assets, m.mu, m.T = BASKET_GBM, len(s), mu, T
+    m.S0, m.S0_vec, m.sigma_vec = float(s[0]), ps, psg
+    keep = [s, sg]
+    if L is None:
+        m.uncorrelated = 1
+    else:
+        la, pl = _arr(L)
+        m.L = pl
+        keep.append(la)
+    if weights is not None:
+        w, pw = _arr(weights)
+        m.weights = pw
+        keep.append(w)
+    return _keep(m, *keep)
+
+
+def localvol_grid(K_axis, t_axis, sigma_grid, S0=100.0, mu=0.05, T=1.0):
+    """sigma_grid[j, i] = sigma(K_i, t_j)."""
+    m = Model()
+    k, pk = _arr(K_axis)
+    t, pt = _arr(t_axis)
+    g, pg = _arr(np.asarray(sigma_grid, dtype=np.float64).reshape(len(t), len(k)))
+    m.kind, m.S0, m.mu, m.T = LOCALVOL_GRID, S0, mu, T
+    m.lv_nK, m.lv_nt, m.lv_K, m.lv_t, m.lv_sigma = len(k), len(t), pk, pt, pg
+    return _keep(m, k, t, g)
+
+
+def payoff(kind, K=100.0, B=0.0, r=0.05, T=1.0, sigma=0.2, n_assets=0):
+    p = Payoff()
+    p.kind, p.K, p.B, p.r, p.T, p.sigma, p.n_assets = kind, K, B, r, T, sigma, n_assets
+    return p
+
+
+def european(K, r, T):
+    return payoff(EUROPEAN, K=K, r=r, T=T)
+
+
+def asian(K):
+    return payoff(ASIAN, K=K)
+
+
+def geom_asian(K):
+    return payoff(GEOM_ASIAN, K=K)
+
+
+def lookback(sigma):
+    return payoff(LOOKBACK, sigma=sigma)
+
+
+def barrier_up_out(K, B, sigma, r, T):
+    return payoff(BARRIER_UP_OUT, K=K, B=B, sigma=sigma, r=r, T=T)
+
+
+def barrier_down_out(K, B, sigma, r, T):
+    return payoff(BARRIER_DOWN_OUT, K=K, B=B, sigma=sigma, r=r, T=T)
+
+
+def basket(K, r, T, n_assets):
+    return payoff(BASKET, K=K, r=r, T=T, n_assets=n_assets)
+
+
+def noise_dim(m):
+    if m.kind == HESTON:
+        return 2
+    if m.kind in (MULTI_DUPIRE, BASKET_GBM):
+        return m.n_assets
+    return 1

@@ -1,0 +1,250 @@
+/*
+ * mcq.h — C ABI of the B200-native MC / RQMC / MLMC / MLQMC pricing engine.
+ *
+ * Every entry point is `extern "C"`, takes plain structs, pointers and sizes, returns an
+ * int status (MCQ_OK == 0) and never lets a C++ exception escape.  On failure the status
+ * is non-zero and mcq_last_error() returns a thread-local message.
+ *
+ * The entry points replace the reference's C++ driver API (methods_cuda.cuh:58-134 of
+ * QuantGuy3/financial-derivatives-montecarlo); each declaration below names the
+ * reference function it stands in for.  include/mcq.hpp layers the reference's own C++
+ * types (ModelVariant, PayoffVariant, MCConfig, ...) over this ABI so that callers of the
+ * reference compile unchanged.
+ *
+ * Conventions
+ *   - Output buffers are caller-owned.  Host pointers unless the name says "device".
+ *   - `stream` arguments are cudaStream_t passed as void*; NULL means the engine's own
+ *     internal stream.
+ *   - The engine uses the CUDA device selected by mcq_init() (default: current device).
+ *   - Not re-entrant per handle: two threads must not share one BB/PCA handle or one
+ *     book object at the same time.  Distinct handles may be used concurrently.
+ */
+#ifndef MCQ_H
+#define MCQ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define MCQ_OK               0
+#define MCQ_ERR_INVALID      1   /* bad argument (size, kind, null pointer)          */
+#define MCQ_ERR_CUDA         2   /* a CUDA runtime call failed                       */
+#define MCQ_ERR_UNSUPPORTED  3   /* combination the engine does not implement        */
+#define MCQ_ERR_RANGE        4   /* Sobol offset beyond 2^32, dimension beyond table */
+#define MCQ_ERR_NOMEM        5   /* device or host allocation failed                 */
+#define MCQ_ERR_INTERNAL     6
+#define MCQ_ERR_TIMEOUT      7   /* a bounded device-side wait gave up               */
+#define MCQ_ERR_CANCELLED    8   /* a book run was cancelled                         */
+
+/* ---------------------------------------------------------------- enumerations */
+/* Model kinds.  0..3 follow ModelKind (methods_cuda.cu:205); 4, 5 are engine additions. */
+#define MCQ_MODEL_GBM            0  /* GBMParams          models.hpp:15-21 */
+#define MCQ_MODEL_HESTON         1  /* HestonParams       models.hpp:23-43 */
+#define MCQ_MODEL_DUPIRE         2  /* DupireLocalParams  models.hpp:45-54 */
+#define MCQ_MODEL_MULTI_DUPIRE   3  /* MultiDupireParams  models.hpp:56-68 */
+#define MCQ_MODEL_LOCALVOL_GRID  4  /* grid local-vol surface, bilinear (new)            */
+#define MCQ_MODEL_BASKET_GBM     5  /* correlated GBM basket, per-asset sigma (new)      */
+
+/* Payoff kinds.  0..5 follow PayoffKind (methods_cuda.cu:202); 6 is an engine addition. */
+#define MCQ_PAYOFF_EUROPEAN          0  /* payoffs.hpp:14 */
+#define MCQ_PAYOFF_ASIAN             1  /* payoffs.hpp:15 (undiscounted, as the reference) */
+#define MCQ_PAYOFF_GEOM_ASIAN        2  /* payoffs.hpp:16 (undiscounted) */
+#define MCQ_PAYOFF_LOOKBACK          3  /* payoffs.hpp:17 floating strike, undiscounted */
+#define MCQ_PAYOFF_BARRIER_UP_OUT    4  /* payoffs.hpp:18 */
+#define MCQ_PAYOFF_BASKET            5  /* payoffs.hpp:19 */
+#define MCQ_PAYOFF_BARRIER_DOWN_OUT  6  /* down-and-out call (new) */
+
+/* Noise transforms (NoiseMode, methods_cuda.cuh:35). */
+#define MCQ_NOISE_RAW  0
+#define MCQ_NOISE_BB   1
+#define MCQ_NOISE_PCA  2
+
+/* Behaviour flags (mcq_qmc_cfg.flags / mcq_mlmc_cfg.flags). */
+#define MCQ_FLAG_COMPAT_U_INF        1  /* keep u = 1.0f -> +inf normal (methods_cuda.cu:823);
+                                           default maps that single float to 1 - 2^-24 */
+#define MCQ_FLAG_COMPAT_HESTON_MLMC  2  /* skip the running (path-dependent) update on the
+                                           Heston coupled path, as methods_cuda.cu:464-490 */
+
+/* ---------------------------------------------------------------- parameter structs */
+typedef struct mcq_model {
+    int32_t kind;                 /* MCQ_MODEL_* */
+    int32_t n_assets;             /* MULTI_DUPIRE / BASKET_GBM */
+    /* common */
+    double S0, mu, T;
+    /* GBM */
+    double sigma;
+    /* Heston: dS = mu S dt + sqrt(v) S dW1, dv = kappa(theta - v) dt + xi sqrt(v) dW2.
+       hes_L10/hes_L11 are the second row of the 2x2 Cholesky factor exactly as
+       HestonParams::L (models.hpp:36-42); mcq_model_heston() fills them from rho. */
+    double kappa, theta, xi, rho, v0, hes_L10, hes_L11;
+    /* parametric Dupire: sigma_loc = sigma0 exp(-alpha t) (S/S0)^(beta_d - 1) */
+    double sigma0, alpha, beta_d;
+    /* multi-asset */
+    int32_t uncorrelated;         /* 1: rho = I, L ignored */
+    int32_t _pad0;
+    const double* S0_vec;         /* [n_assets] */
+    const double* L;              /* [n_assets * n_assets] row-major lower Cholesky */
+    const double* sigma_vec;      /* [n_assets] BASKET_GBM */
+    const double* weights;        /* [n_assets] BASKET_GBM (NULL: equal weights) */
+    /* local-vol grid: sigma(K_i, t_j) at lv_sigma[j * lv_nK + i] */
+    int32_t lv_nK, lv_nt;
+    const double* lv_K;           /* [lv_nK] increasing */
+    const double* lv_t;           /* [lv_nt] increasing */
+    const double* lv_sigma;       /* [lv_nt * lv_nK] */
+} mcq_model;
+
+typedef struct mcq_payoff {
+    int32_t kind;                 /* MCQ_PAYOFF_* */
+    int32_t n_assets;             /* Basket{... n_assets} */
+    double K, B, r, T, sigma;     /* sigma: BGK continuity-correction volatility (Lookback, Barrier) */
+} mcq_payoff;
+
+/* MCConfig (methods_cuda.cuh:10-14). */
+typedef struct mcq_mc_cfg {
+    int64_t  N_batch;             /* default 1<<16; only bounds host bookkeeping here */
+    int32_t  pilot_n;             /* default 10000 */
+    uint32_t seed;                /* default 123 */
+} mcq_mc_cfg;
+
+/* QMCConfig (methods_cuda.cuh:16-26) plus the values the reference hard-codes. */
+typedef struct mcq_qmc_cfg {
+    int32_t  R;                   /* default 32 replicas */
+    int32_t  max_doublings;       /* default 20 */
+    int64_t  N0_per_replica;      /* 0: the reference's memory-derived start (methods_cuda.cu:1523-1533) */
+    uint32_t salt_base;           /* default 42 (methods_cuda.cu:1564) */
+    int32_t  flags;               /* MCQ_FLAG_* */
+} mcq_qmc_cfg;
+
+/* MLMCConfig (methods_cuda.cuh:28-32) plus the level-0 step count. */
+typedef struct mcq_mlmc_cfg {
+    int32_t M;                    /* default 2 */
+    int32_t max_L;                /* default 10 */
+    int32_t pilot_n;              /* default 400 */
+    int32_t n0_steps;             /* steps on level 0; the reference uses 1 (methods_cuda.cu:1349) */
+    int32_t flags;                /* MCQ_FLAG_* */
+    uint32_t seed;                /* MLMC pseudo-random stream base; default 42 (methods_cuda.cu:1412) */
+} mcq_mlmc_cfg;
+
+/* MCResult (methods_cuda.cuh:42-47) plus work accounting. */
+typedef struct mcq_result {
+    double  price;
+    double  std_error;
+    int64_t n_samples;
+    double  time_s;
+    double  path_steps;           /* total simulated path-steps (fine + coarse for MLMC) */
+    int32_t levels;               /* MLMC/MLQMC: L + 1 */
+    int32_t launches;             /* engine kernel launches issued */
+} mcq_result;
+
+/* CVPilot (methods_cuda.cuh:94). */
+typedef struct mcq_cv_pilot_out { double beta, var_plain, var_cv; } mcq_cv_pilot_out;
+
+typedef struct mcq_handle_s* mcq_handle;   /* opaque BB / PCA handle */
+
+/* ---------------------------------------------------------------- lifecycle */
+int         mcq_init(int device);          /* -1: current device */
+int         mcq_shutdown(void);
+const char* mcq_last_error(void);
+int         mcq_version(void);             /* major*10000 + minor*100 + patch */
+int         mcq_default_cfgs(mcq_mc_cfg* mc, mcq_qmc_cfg* qmc, mcq_mlmc_cfg* ml);
+int         mcq_model_heston(double S0, double mu, double kappa, double theta, double xi,
+                             double rho, double v0, double T, mcq_model* out);
+
+/* ---------------------------------------------------------------- BB / PCA handles
+ * mcq_bb_create   replaces bb_precompute + bb_upload   (utils.cpp:54-101, methods_cuda.cu:928-953)
+ * mcq_pca_create  replaces pca_compute  + pca_upload   (utils.cpp:131-167, methods_cuda.cu:962-971)
+ * mcq_pca_create_from uploads a caller-supplied m x m column-major M_pca.
+ * mcq_handle_free replaces bb_free / pca_free          (methods_cuda.cu:955-977) */
+int mcq_bb_create(int N, double T, mcq_handle* out);
+int mcq_pca_create(int m, double T, mcq_handle* out);
+int mcq_pca_create_from(int m, double T, const double* M_pca_colmajor, mcq_handle* out);
+int mcq_handle_free(mcq_handle h);
+int mcq_handle_info(mcq_handle h, int* kind, int* n);
+
+/* ---------------------------------------------------------------- estimator drivers */
+/* run_mc_cuda (methods_cuda.cu:1272-1298): pilot, N = 2 Var / eps^2, main run. */
+int mcq_run_mc(const mcq_model* m, const mcq_payoff* p, double eps, int n_steps,
+               const mcq_mc_cfg* cfg, mcq_result* out);
+/* run_mc_fixed (methods_cuda.cu:2368-2374): mean and variance of the mean of n_paths. */
+int mcq_run_mc_fixed(const mcq_model* m, const mcq_payoff* p, int n_steps, int64_t n_paths,
+                     uint32_t seed, double* mean, double* var_of_mean);
+/* run_qmc_cuda (methods_cuda.cu:1494-1673): R scrambled replicas, doubling. */
+int mcq_run_qmc(const mcq_model* m, const mcq_payoff* p, double eps, int n_steps,
+                const mcq_qmc_cfg* cfg, int noise_mode, mcq_handle bb, mcq_handle pca,
+                mcq_result* out);
+/* run_mlmc_cuda (methods_cuda.cu:1305-1487). */
+int mcq_run_mlmc(const mcq_model* m, const mcq_payoff* p, double eps,
+                 const mcq_mlmc_cfg* cfg, mcq_result* out);
+/* run_mlqmc_cuda (methods_cuda.cu:1680-2019); bb_list/pca_list: one handle per level. */
+int mcq_run_mlqmc(const mcq_model* m, const mcq_payoff* p, double eps,
+                  const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qmc, int noise_mode,
+                  const mcq_handle* bb_list, int n_bb, const mcq_handle* pca_list, int n_pca,
+                  mcq_result* out);
+/* cv_pilot (methods_cuda.cu:2026-2076). */
+int mcq_cv_pilot(const mcq_model* main_m, const mcq_model* ctrl_m, const mcq_payoff* main_p,
+                 const mcq_payoff* ctrl_p, double E_ctrl, int n_steps, int N_pilot,
+                 uint32_t seed, mcq_cv_pilot_out* out);
+/* run_mc_cv_cuda (methods_cuda.cu:2078-2163). */
+int mcq_run_mc_cv(const mcq_model* main_m, const mcq_model* ctrl_m, const mcq_payoff* main_p,
+                  const mcq_payoff* ctrl_p, double E_ctrl, double beta, double eps, int n_steps,
+                  const mcq_mc_cfg* cfg, mcq_result* out);
+/* run_qmc_cv_cuda (methods_cuda.cu:2165-2278). */
+int mcq_run_qmc_cv(const mcq_model* main_m, const mcq_model* ctrl_m, const mcq_payoff* main_p,
+                   const mcq_payoff* ctrl_p, double E_ctrl, double beta, double eps, int n_steps,
+                   const mcq_qmc_cfg* cfg, mcq_result* out);
+/* run_is_cuda (methods_cuda.cu:2285-2365): GBM European with drift shift z_star. */
+int mcq_run_is(const mcq_model* gbm, const mcq_payoff* european, double z_star, double eps,
+               const mcq_mc_cfg* cfg, mcq_result* out);
+
+/* ---------------------------------------------------------------- hot-path passes
+ * One fused kernel pass over R replicas x n_points scrambled-Sobol points (salts
+ * salt_base + r, point indices offset .. offset + n_points - 1).  sums_host receives
+ * [R][2] doubles {sum Y, sum Y^2}.  This is the unit the QMC driver repeats per doubling
+ * (accumulate_range, methods_cuda.cu:1549-1622, with no D x N array). */
+int mcq_qmc_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, int noise_mode,
+                 mcq_handle bb, mcq_handle pca, uint32_t salt_base, int R, uint32_t offset,
+                 int64_t n_points, int flags, double* sums_host);
+/* Same pass with device-resident output (sums_device: R*2 doubles) on `stream`;
+   asynchronous.  Used to time the kernel with inputs and outputs resident in HBM. */
+int mcq_qmc_pass_device(const mcq_model* m, const mcq_payoff* p, int n_steps, int noise_mode,
+                        mcq_handle bb, mcq_handle pca, uint32_t salt_base, int R,
+                        uint32_t offset, int64_t n_points, int flags, double* sums_device,
+                        void* stream);
+/* Pseudo-random (Philox4x32-10) pass over n_paths paths of stream `stream_id`, starting
+   at path index first_path: sums_host[2] = {sum Y, sum Y^2}.  The unit behind run_mc. */
+int mcq_mc_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t seed,
+                uint32_t stream_id, int64_t first_path, int64_t n_paths, double* sums_host);
+/* Coupled fine/coarse level pass (kernel_mlmc, methods_cuda.cu:445-518): sums_host receives
+   [R][4] = {sum dY, sum dY^2, sum Yf, sum Yf^2}.  use_sobol=1: salts salt_base + r and
+   offset; use_sobol=0: Philox with key `seed`, stream salt_base + r, paths from offset. */
+int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, int noise_mode,
+                   mcq_handle bb, mcq_handle pca, int use_sobol, uint32_t seed,
+                   uint32_t salt_base, int R, uint32_t offset, int64_t n_points, int flags,
+                   double* sums_host);
+
+/* ---------------------------------------------------------------- parity / debug exports
+ * Hong–Hickernell scrambled Sobol stream (methods_cuda.cu:753-825): out[d * n + i] for
+ * dimension dim0 + d and point index offset + i.  _u32 returns the scrambled integers,
+ * _normal the N(0,1) values the path kernels consume. */
+int mcq_sobol_hh_u32(uint32_t salt, int dim0, int nd, uint32_t offset, int64_t n,
+                     uint32_t* out_host);
+int mcq_sobol_hh_normal(uint32_t salt, int dim0, int nd, uint32_t offset, int64_t n,
+                        int flags, float* out_host);
+/* Philox4x32-10 block (counter, key) -> 4 words; host-side, for known-answer checks. */
+int mcq_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* BB / PCA tables as the device sees them (for parity tests). */
+int mcq_bb_tables(mcq_handle bb, int* map_idx, float* wl, float* wr, float* sd);  /* per dimension */
+int mcq_pca_matrix(mcq_handle pca, float* M_colmajor_f32);
+/* The normals (raw) or time-ordered increments (bridge) that one fused pass consumed, for
+   bit-level parity tests: out_host[R][n_points][n_steps * d_noise].  n_points <= 2^20. */
+int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_handle bb,
+                        int use_sobol, uint32_t seed, uint32_t salt_base, int R, uint32_t offset,
+                        int64_t n_points, int flags, float* out_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCQ_H */

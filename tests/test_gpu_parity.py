@@ -1,0 +1,148 @@
+"""Fused pass sums vs the FP64 oracle on the same points, for every model x payoff the
+reference supports (plus the down-and-out barrier and the grid local-vol model).
+
+Tolerance: the engine steps paths in FP32 (as the reference) and the oracle in FP64 on the
+same normals, so per-replica means agree to ~1e-5 relative; barrier payoffs may flip a
+knock-out decision for a path whose extremum sits within FP32 rounding of the barrier, which
+moves a mean by at most (max payoff)/N — that bound is added for barrier payoffs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PAYOFFS = ["eur", "asian", "geom", "lookback", "upout", "downout"]
+
+
+def make_payoff(eng, name, T=1.0):
+    return {
+        "eur": lambda: eng.european(100.0, 0.05, T),
+        "asian": lambda: eng.asian(100.0),
+        "geom": lambda: eng.geom_asian(100.0),
+        "lookback": lambda: eng.lookback(0.2),
+        "upout": lambda: eng.barrier_up_out(100.0, 125.0, 0.2, 0.05, T),
+        "downout": lambda: eng.barrier_down_out(100.0, 85.0, 0.2, 0.05, T),
+    }[name]()
+
+
+def make_model(eng, name):
+    if name == "gbm":
+        return eng.gbm(100.0, 0.05, 0.2, 1.0)
+    if name == "heston":
+        return eng.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)
+    if name == "dupire":
+        return eng.dupire(100.0, 0.05, 0.2, 0.5, 0.7, 1.0)
+    if name == "lv":
+        K = np.linspace(50, 150, 64)
+        t = np.linspace(0, 2, 32)
+        g = 0.2 + 0.1 * np.exp(-(K[None, :] / 100 - 1) ** 2 / 0.05) * (1 + 0.5 * t[:, None])
+        return eng.localvol_grid(K, t, g, 100.0, 0.05, 1.0)
+    raise ValueError(name)
+
+
+def tol(pay, N, mean):
+    t = 2e-4 * (1 + abs(mean))
+    if pay in ("upout", "downout"):
+        t += 60.0 / N
+    return t
+
+
+@pytest.mark.parametrize("model", ["gbm", "heston", "dupire", "lv"])
+@pytest.mark.parametrize("pay", PAYOFFS)
+def test_qmc_pass_raw(gpu, orc, model, pay):
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    n_steps, R, N, off = 24, 2, 640, 13
+    g = gpu.qmc_pass(m, p, n_steps, salt_base=42, R=R, offset=off, n_points=N)
+    o = orc.qmc_sums(m, p, n_steps, None, salt_base=42, R=R, offset=off, N=N)
+    for r in range(R):
+        assert abs(g[r, 0] / N - o[r, 0] / N) < tol(pay, N, o[r, 0] / N), (r, g[r], o[r])
+        assert abs(g[r, 1] - o[r, 1]) < 1e-3 * (1 + abs(o[r, 1])) + (4000.0 if pay in ("upout", "downout") else 0)
+
+
+@pytest.mark.parametrize("model", ["gbm", "dupire", "lv"])
+@pytest.mark.parametrize("pay", ["eur", "asian", "lookback", "downout"])
+@pytest.mark.parametrize("N_steps", [16, 64])
+def test_qmc_pass_bridge(gpu, orc, model, pay, N_steps):
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    bb = gpu.bb_create(N_steps, 1.0)
+    R, N = 2, 512
+    g = gpu.qmc_pass(m, p, N_steps, noise=gpu.BB, bb=bb, salt_base=77, R=R, offset=64, n_points=N)
+    o = orc.qmc_sums(m, p, N_steps, orc.noise(orc.T.BB, N_steps, 1.0), salt_base=77, R=R, offset=64, N=N)
+    for r in range(R):
+        assert abs(g[r, 0] / N - o[r, 0] / N) < tol(pay, N, o[r, 0] / N), (r, g[r], o[r])
+    bb.close()
+
+
+@pytest.mark.parametrize("model", ["gbm", "heston", "dupire"])
+@pytest.mark.parametrize("pay", ["eur", "asian", "lookback", "downout"])
+@pytest.mark.parametrize("level", [0, 1, 3])
+@pytest.mark.parametrize("M", [2, 4])
+def test_level_pass(gpu, orc, model, pay, level, M):
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    n0 = 1 if M == 2 else 4
+    n_fine = n0 * M ** level
+    Mp = M if level > 0 else 0
+    R, N = 2, 384
+    for use_sobol in (True, False):
+        g = gpu.level_pass(m, p, n_fine, Mp, use_sobol=use_sobol, seed=42, salt_base=90, R=R, offset=5, n_points=N)
+        o = orc.level_sums(m, p, n_fine, Mp, None, use_sobol=use_sobol, seed=42, salt_base=90, R=R, offset=5, N=N)
+        for r in range(R):
+            for k in (0, 2):
+                assert abs(g[r, k] / N - o[r, k] / N) < tol(pay, N, o[r, k] / N) * 2, (use_sobol, r, k, g[r], o[r])
+
+
+def test_heston_mlmc_compat_flag_skips_running_update(gpu, orc):
+    m, p = make_model(gpu, "heston"), make_payoff(gpu, "lookback")
+    N = 256
+    for flags in (0, gpu.FLAG_COMPAT_HESTON_MLMC):
+        g = gpu.level_pass(m, p, 16, 4, use_sobol=True, salt_base=3, R=1, n_points=N, flags=flags)
+        o = orc.level_sums(m, p, 16, 4, None, use_sobol=True, salt_base=3, R=1, N=N, flags=flags)
+        assert abs(g[0, 2] / N - o[0, 2] / N) < 1e-3, flags
+
+
+@pytest.mark.parametrize("model,pay", [("gbm", "eur"), ("heston", "asian"), ("dupire", "lookback"), ("lv", "geom")])
+def test_mc_pass_philox(gpu, orc, model, pay):
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    N = 700
+    g = gpu.mc_pass(m, p, 40, 123, 5, 1000, N)
+    o = orc.mc_sums(m, p, 40, 123, 5, 1000, N)
+    assert abs(g[0] / N - o[0] / N) < 2e-4 * (1 + abs(o[0] / N)), (g, o)
+
+
+@pytest.mark.parametrize("kind", ["multi", "basket"])
+@pytest.mark.parametrize("n", [1, 3, 8, 16])
+def test_basket_pass(gpu, orc, kind, n):
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n))
+    Cm = A @ A.T + 0.5 * np.eye(n)
+    d = np.sqrt(np.diag(Cm))
+    L = np.linalg.cholesky(Cm / np.outer(d, d))
+    S0 = 100 * rng.uniform(0.8, 1.2, n)
+    if kind == "multi":
+        m = gpu.multi_dupire(S0, L)
+    else:
+        m = gpu.basket_gbm(S0, rng.uniform(0.1, 0.5, n), L, rng.dirichlet(np.ones(n)))
+    p = gpu.basket(100.0, 0.05, 1.0, n)
+    R, N, steps = 2, 256, 12
+    g = gpu.qmc_pass(m, p, steps, salt_base=11, R=R, offset=3, n_points=N)
+    o = orc.qmc_sums(m, p, steps, None, salt_base=11, R=R, offset=3, N=N)
+    for r in range(R):
+        assert abs(g[r, 0] / N - o[r, 0] / N) < 3e-4 * (1 + abs(o[r, 0] / N)), (r, g[r], o[r])
+
+
+def test_cv_pilot_matches_pathwise_oracle(gpu, orc):
+    m = gpu.gbm(100.0, 0.05, 0.2, 1.0)
+    pa, pg = gpu.asian(100.0), gpu.geom_asian(100.0)
+    n_steps, N, seed = 16, 1500, 7
+    E = orc.geom_asian(100, 100, 1, 0.05, 0.2, n_steps)
+    got = gpu.cv_pilot(m, m, pa, pg, E, n_steps, N, seed)
+    ya, yg = [], []
+    for i in range(N):
+        z = orc.philox_normals(seed, 0, i, n_steps)
+        ya.append(orc.path_payoff(m, pa, n_steps, z))
+        yg.append(orc.path_payoff(m, pg, n_steps, z))
+    ya, yg = np.array(ya), np.array(yg)
+    va = ya.var()
+    vg = max(1e-30, yg.var())
+    cov = (ya * yg).mean() - ya.mean() * yg.mean()
+    assert abs(got["var_plain"] - va) < 1e-4 * va
+    assert abs(got["beta"] - np.clip(cov / vg, 0, 5)) < 1e-4
