@@ -6,7 +6,7 @@ GBM, S0 = K = 100, r = mu = 0.03, sigma = 0.25, T = 1, 256 Euler steps = 256 Hon
 scrambled Sobol dimensions, R = 32 replicas with salts 42.., raw noise ordering.
 
   value  one "step" = one fused pass over 32 replicas x N points x 256 steps (default
-         N = 2^18 per replica, 2.1e9 path-steps), inputs (direction tables, parameters)
+         N = 2^20 per replica, 8.6e9 path-steps), inputs (direction tables, parameters)
          resident, sums left on the device; device time from CUDA events on the launching
          stream; L2 flushed (256 MiB write) between steps.
   e2e    the reference-facing driver call mcq_run_qmc (run_qmc_cuda's entry point) at
@@ -54,7 +54,7 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -66,7 +66,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -161,7 +161,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--points", type=int, default=1 << 18, help="points per replica per step")
+    ap.add_argument("--points", type=int, default=1 << 20, help="points per replica per step")
     ap.add_argument("--e2e-runs", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -184,8 +184,12 @@ def main():
     N = args.points
     sums = torch.zeros(REPS * 2, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: torch's default stream has handle 0, which the C ABI reads as "use
+    # the engine's internal stream", and the events below must sit on the launching stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
+    assert sp != 0
 
     def one_pass():
         eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, salt_base=salt, R=REPS, offset=0, n_points=N)

@@ -207,9 +207,11 @@ __host__ __device__ constexpr bool path_dep() {
 }
 
 // One discretisation of one single-asset path (d_euler_gbm / d_euler_heston / d_euler_dupire
-// and d_running_* / d_apply_bgk / d_payoff, methods_cuda.cu:270-352).  The Euler updates are
-// written as S * (1 + mu h + vol dW); the reference's S + mu S h + vol S dW differs only in
-// rounding.
+// and d_running_* / d_apply_bgk / d_payoff, methods_cuda.cu:270-352).  The Euler update is
+// S + S (mu h + vol dW), two FMAs; the reference's S + mu S h + vol S dW differs only in
+// rounding.  (Folding the drift into a constant 1 + mu h would round that constant once and
+// repeat the same relative error on every step: a systematic drift bias of up to 3e-4 of
+// mu h per step that does not cancel between the fine and coarse paths of an MLMC level.)
 template <int MOD, int PAY>
 struct Leg {
     float S, V, r0, r1;
@@ -225,18 +227,18 @@ struct Leg {
     }
     template <bool RUN>
     __device__ __forceinline__ void step(const KParams& p, float dw1, float dw2, float t,
-                                         float omh, float em) {
+                                         float muh, float em) {
         if constexpr (MOD == MOD_GBM) {
-            S = S * fmaf(p.sigma, dw1, omh);
+            S = fmaf(S, fmaf(p.sigma, dw1, muh), S);
         } else if constexpr (MOD == MOD_DUPIRE) {
             const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S * p.inv_S0), -p.alpha * t * kLog2e));
-            S = S * fmaf(sl, dw1, omh);
+            S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_LVGRID) {
             const float sl = lv_sigma(p, S, t);
-            S = S * fmaf(sl, dw1, omh);
+            S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_HESTON) {
             const float sq = sqrtf(fmaxf(V, 0.f));
-            S = S * fmaf(sq, dw1, omh);
+            S = fmaf(S, fmaf(sq, dw1, muh), S);
             V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
         }
         if constexpr (RUN && path_dep<PAY>()) update();
@@ -262,28 +264,28 @@ struct PathC {
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr bool HES = (MOD == MOD_HESTON);
     Leg<MOD, PAY> f, c;
-    float a1, a2, omh_f, omh_c;
+    float a1, a2, muh_f, muh_c;   // mu h of the fine and coarse steps
     int k, m, ck;
     bool run_upd;
     __device__ __forceinline__ void init(const KParams& p) {
         f.init(p);
-        omh_f = fmaf(p.mu, p.h, 1.0f);
+        muh_f = p.mu * p.h;
         k = 0;
         run_upd = !(HES && COUPLED && (p.flags & 2));
-        if constexpr (COUPLED) { c.init(p); a1 = a2 = 0.f; m = 0; ck = 0; omh_c = fmaf(p.mu, p.hc, 1.0f); }
+        if constexpr (COUPLED) { c.init(p); a1 = a2 = 0.f; m = 0; ck = 0; muh_c = p.mu * p.hc; }
     }
     __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
         const float t = (float)k * p.h;
-        if (run_upd) f.template step<true>(p, dw1, dw2, t, omh_f, p.em_f);
-        else f.template step<false>(p, dw1, dw2, t, omh_f, p.em_f);
+        if (run_upd) f.template step<true>(p, dw1, dw2, t, muh_f, p.em_f);
+        else f.template step<false>(p, dw1, dw2, t, muh_f, p.em_f);
         k++;
         if constexpr (COUPLED) {
             a1 += dw1;
             if constexpr (HES) a2 += dw2;
             if (++m == p.M) {
                 const float tc = (float)ck * p.hc;
-                if (run_upd) c.template step<true>(p, a1, a2, tc, omh_c, p.em_c);
-                else c.template step<false>(p, a1, a2, tc, omh_c, p.em_c);
+                if (run_upd) c.template step<true>(p, a1, a2, tc, muh_c, p.em_c);
+                else c.template step<false>(p, a1, a2, tc, muh_c, p.em_c);
                 a1 = a2 = 0.f; m = 0; ck++;
             }
         }
@@ -320,12 +322,12 @@ struct PathC {
 struct CvAsianC {
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr int NST = 7;
-    float S, sa, ca, sl, cl, omh;
+    float S, sa, ca, sl, cl, muh;
     __device__ __forceinline__ void init(const KParams& p) {
-        S = p.S0; sa = ca = sl = cl = 0.f; omh = fmaf(p.mu, p.h, 1.0f);
+        S = p.S0; sa = ca = sl = cl = 0.f; muh = p.mu * p.h;
     }
     __device__ __forceinline__ void step_dw(const KParams& p, float dw, float) {
-        S = S * fmaf(p.sigma, dw, omh);
+        S = fmaf(S, fmaf(p.sigma, dw, muh), S);
         kadd(sa, ca, S);
         kadd(sl, cl, logf(S));
     }
@@ -349,16 +351,16 @@ struct CvAsianC {
 struct CvDupireC {
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr int NST = 7;
-    float Sd, Sg, omh;
+    float Sd, Sg, muh;
     int k;
     __device__ __forceinline__ void init(const KParams& p) {
-        Sd = Sg = p.S0; omh = fmaf(p.mu, p.h, 1.0f); k = 0;
+        Sd = Sg = p.S0; muh = p.mu * p.h; k = 0;
     }
     __device__ __forceinline__ void step_dw(const KParams& p, float dw, float) {
         const float t = (float)k * p.h;
         const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(Sd * p.inv_S0), -p.alpha * t * kLog2e));
-        Sd = Sd * fmaf(sl, dw, omh);
-        Sg = Sg * fmaf(p.ctrl_sigma, dw, omh);
+        Sd = fmaf(Sd, fmaf(sl, dw, muh), Sd);
+        Sg = fmaf(Sg, fmaf(p.ctrl_sigma, dw, muh), Sg);
         k++;
     }
     __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
@@ -380,16 +382,16 @@ struct CvDupireC {
 struct IsC {
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr int NST = 2;
-    float S, zs, zc, omh;
+    float S, zs, zc, muh;
     __device__ __forceinline__ void init(const KParams& p) {
-        S = p.S0; zs = zc = 0.f; omh = fmaf(p.mu, p.h, 1.0f);
+        S = p.S0; zs = zc = 0.f; muh = p.mu * p.h;
     }
     __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
 #pragma unroll
         for (int i = 0; i < 32; i++)
             if (i < nv) {
                 kadd(zs, zc, z[i]);
-                S = S * fmaf(p.sigma, (z[i] + p.z_star) * p.sqrt_h, omh);
+                S = fmaf(S, fmaf(p.sigma, (z[i] + p.z_star) * p.sqrt_h, muh), S);
             }
     }
     __device__ __forceinline__ void step_dw(const KParams&, float, float) {}
@@ -409,13 +411,13 @@ struct BasketC {
     static constexpr int NST = 2;
     __device__ __forceinline__ void bind(int, uint64_t) {}
     float S[NB], dw[NB];
-    float omh;
+    float muh;
     int f, k;
     __device__ __forceinline__ void init(const KParams& p) {
         const int n = p.n_assets;
 #pragma unroll
         for (int a = 0; a < NB; a++) { S[a] = (a < n) ? __ldg(p.bsk + a) : 0.f; dw[a] = 0.f; }
-        omh = fmaf(p.mu, p.h, 1.0f);
+        muh = p.mu * p.h;
         f = 0; k = 0;
     }
     __device__ __forceinline__ void feed(const KParams& p, float z) {
@@ -437,9 +439,9 @@ struct BasketC {
                 if (a < n) {
                     if constexpr (MOD == MOD_MULTI) {
                         const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * p.inv_S0), -p.alpha * t * kLog2e));
-                        S[a] = S[a] * fmaf(sl, dw[a], omh);
+                        S[a] = fmaf(S[a], fmaf(sl, dw[a], muh), S[a]);
                     } else {
-                        S[a] = S[a] * fmaf(__ldg(p.bsk + n + a), dw[a], omh);
+                        S[a] = fmaf(S[a], fmaf(__ldg(p.bsk + n + a), dw[a], muh), S[a]);
                     }
                 }
                 dw[a] = 0.f;
