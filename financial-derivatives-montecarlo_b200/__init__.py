@@ -26,7 +26,7 @@ EXPORTS = [
     "mcq_run_mc", "mcq_run_mc_fixed", "mcq_run_qmc", "mcq_run_mlmc", "mcq_run_mlqmc", "mcq_cv_pilot",
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
     "mcq_mc_pass", "mcq_level_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
-    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump",
+    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_qmc_pass_noalloc",
 ]
 
 
@@ -229,6 +229,14 @@ def qmc_pass_device(m, p, n_steps, sums_device_ptr, stream_ptr=0, noise=RAW, bb=
     _check(lib().mcq_qmc_pass_device(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_int(noise), _h(bb), _h(pca),
                                      C.c_uint32(salt_base), C.c_int(R), C.c_uint32(offset), C.c_int64(n_points),
                                      C.c_int(flags), C.c_void_p(sums_device_ptr), C.c_void_p(stream_ptr)))
+
+
+def qmc_pass_noalloc(m, p, n_steps, sums_device_ptr, stream_ptr=0, salt_base=42, R=1, offset=0, n_points=1024,
+                     flags=0):
+    """mcq_qmc_pass_noalloc: the RQMC pass with all scratch in the library's fixed device array."""
+    _check(lib().mcq_qmc_pass_noalloc(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_uint32(salt_base), C.c_int(R),
+                                      C.c_uint32(offset), C.c_int64(n_points), C.c_int(flags),
+                                      C.c_void_p(sums_device_ptr), C.c_void_p(stream_ptr)))
 
 
 def mc_pass(m, p, n_steps, seed, stream_id, first_path, n_paths):

@@ -16,6 +16,10 @@ using namespace mcq;
 
 static thread_local std::string g_last_error;
 
+namespace mcq {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace mcq
+
 #define API_BEGIN                                   \
     try {                                           \
         std::lock_guard<std::mutex> lk_(engine().mu);

@@ -158,7 +158,7 @@ static bool uniform_axis(const double* a, int n, double* a0, double* inv_d) {
 }
 
 // make_params (methods_cuda.cu:986-1053) in the engine's layout; aux arrays are staged in `ws`.
-static void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
+void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
     const mcq_model& m = *a.m;
     const mcq_payoff& p = *a.p;
     std::memset(&k, 0, sizeof(k));
@@ -276,7 +276,6 @@ static void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
 
 // ------------------------------------------------------------------ launcher
 
-static constexpr long long kTargetItems = 148LL * 16 * 6;   // fixed -> device-independent split
 
 static KernelInfo& kernel_info(const void* fn, size_t smem) {
     Engine& E = engine();

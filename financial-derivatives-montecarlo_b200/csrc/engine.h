@@ -115,12 +115,20 @@ struct PassArgs {
     bool dump = false;
 };
 
+// Work items per pass are sized from the problem alone (never from the device) so that the
+// split, and with it every sum, is the same on any GPU.
+inline constexpr long long kTargetItems = 148LL * 16 * 6;
+
 int noise_dim(const mcq_model& m);
+// KParams for a pass (make_params); basket / local-vol arrays are uploaded into ws.aux.
+void fill_params(Workspace& ws, const PassArgs& a, KParams& k);
 int nstat_of(int est);
 // Enqueue one pass on ws.stream; d_out receives [R][nstat] doubles (device).
 void pass_async(Workspace& ws, const PassArgs& a, double* d_out);
 // Enqueue, copy back and wait; returns [R][nstat].
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
+// Message returned by mcq_last_error() on this thread.
+void set_last_error(const std::string& msg);
 // Device capacity used by the reference's memory-derived batch sizing.
 long long gpu_free_bytes_80();
 

@@ -225,6 +225,21 @@ int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, i
                    uint32_t salt_base, int R, uint32_t offset, int64_t n_points, int flags,
                    double* sums_host);
 
+/* One RQMC pass (as mcq_qmc_pass_device) that allocates no device memory.  No counterpart in
+ * the reference.  For callers that may not call cudaMalloc: code living in a process whose GPU
+ * memory belongs to another allocator (a framework's caching allocator, a plugin host with a
+ * fixed budget) and latency-critical paths where cudaMalloc / cudaFree would synchronise the
+ * device.  Its scratch is one fixed __device__ array inside the library (about 2.4 MiB, held on
+ * every GPU that loads the library until exit); sums_device ([R][2] doubles) is the caller's.
+ * Limits: GBM, Heston or parametric Dupire, raw ordering, n_steps x factors <= 512, R <= 32;
+ * larger requests fail with MCQ_ERR_RANGE.  The first call on a device sets the array up
+ * (resolves its address, loads the direction table with a synchronous copy) and should come
+ * before any stream capture.  All calls share the array: calls that overlap on the GPU race,
+ * so keep them on one stream.  Asynchronous on `stream` (NULL: the legacy default stream). */
+int mcq_qmc_pass_noalloc(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t salt_base,
+                         int R, uint32_t offset, int64_t n_points, int flags, double* sums_device,
+                         void* stream);
+
 /* ---------------------------------------------------------------- parity / debug exports
  * Hong–Hickernell scrambled Sobol stream (methods_cuda.cu:753-825): out[d * n + i] for
  * dimension dim0 + d and point index offset + i.  _u32 returns the scrambled integers,
