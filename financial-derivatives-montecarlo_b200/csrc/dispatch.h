@@ -7,12 +7,23 @@
 namespace mcq {
 
 const void* lookup_sobol_raw_plain(int model, int payoff);
+const void* lookup_sobol_raw_plain_b4(int model, int payoff);   // 64-register variant
 const void* lookup_sobol_raw_coupled(int model, int payoff);
 const void* lookup_sobol_bb(int model, int payoff, bool coupled);
 const void* lookup_philox_plain(int model, int payoff);
 const void* lookup_philox_coupled(int model, int payoff);
 // est in {EST_CV_ASIAN, EST_CV_DUPIRE, EST_IS}, basket models (nb = 4, 8, 16), dump probes
 const void* lookup_misc(int gen, int noise, int est, int model, int nb, bool dump);
+
+// Kernel families with more than one compiled launch variant (see the autotuner in engine.cpp).
+inline int n_variants(int gen, int noise, int est, int model) {
+    return (gen == GEN_SOBOL && noise == NOISE_RAW && est == EST_PLAIN && model != MOD_MULTI &&
+            model != MOD_BASKET) ? 2 : 1;
+}
+inline const void* lookup_variant(int gen, int noise, int est, int model, int payoff, int variant) {
+    if (variant == 1 && n_variants(gen, noise, est, model) == 2) return lookup_sobol_raw_plain_b4(model, payoff);
+    return nullptr;
+}
 
 inline const void* lookup_pass(int gen, int noise, int est, int model, int payoff, int nb) {
     if (model == MOD_MULTI || model == MOD_BASKET || est >= EST_CV_ASIAN)

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "dispatch.h"
@@ -101,6 +102,11 @@ void shutdown_engine() {
     cudaDeviceSynchronize();
     E.pool.clear();
     E.kinfo.clear();
+    for (auto& kv : E.tune)
+        for (auto& pr : kv.second.ev)
+            for (auto& ev : pr)
+                if (ev) cudaEventDestroy(ev);
+    E.tune.clear();
     if (E.d_dv) cudaFree(E.d_dv);
     E.d_dv = nullptr;
     E.ready = false;
@@ -325,6 +331,49 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
 
     const void* fn = a.dump ? lookup_misc(a.gen, a.noise, a.est, k.model, nb, true)
                             : lookup_pass(a.gen, a.noise, a.est, k.model, a.p->kind, nb);
+    // launch variant: MCQ_TUNE=<v> forces one; otherwise the autotuner picks per family
+    int variant = 0;
+    TuneState* trial = nullptr;
+    const int nvar = a.dump ? 1 : n_variants(a.gen, a.noise, a.est, k.model);
+    if (nvar > 1) {
+        const char* force = std::getenv("MCQ_TUNE");
+        if (force) {
+            variant = std::min(std::max(std::atoi(force), 0), nvar - 1);
+        } else {
+            const uint64_t key = (uint64_t)a.gen | ((uint64_t)a.noise << 4) | ((uint64_t)a.est << 8) |
+                                 ((uint64_t)k.model << 12) | ((uint64_t)a.p->kind << 16);
+            TuneState& ts = E.tune[key];
+            for (int v = 0; v < 2; v++) {
+                if (ts.pending[v]) {
+                    float ms = 0.f;
+                    MCQ_CUDA(cudaEventSynchronize(ts.ev[v][1]));
+                    MCQ_CUDA(cudaEventElapsedTime(&ms, ts.ev[v][0], ts.ev[v][1]));
+                    ts.per_unit[v] = ms / ts.units[v];
+                    ts.pending[v] = false;
+                    ts.done[v] = true;
+                }
+            }
+            if (ts.chosen < 0 && ts.done[0] && ts.done[1])
+                ts.chosen = ts.per_unit[1] < ts.per_unit[0] ? 1 : 0;
+            const double units = (double)a.R * (double)a.n_points * (double)k.D;
+            if (ts.chosen >= 0) {
+                variant = ts.chosen;
+            } else if (units >= (double)(1 << 26)) {
+                const int v = !ts.done[0] ? 0 : 1;
+                if (!ts.pending[v]) {
+                    if (!ts.ev[v][0]) {
+                        MCQ_CUDA(cudaEventCreate(&ts.ev[v][0]));
+                        MCQ_CUDA(cudaEventCreate(&ts.ev[v][1]));
+                    }
+                    variant = v;
+                    ts.units[v] = units;
+                    ts.pending[v] = true;
+                    trial = &ts;
+                }
+            }
+        }
+        if (variant > 0) fn = lookup_variant(a.gen, a.noise, a.est, k.model, a.p->kind, variant);
+    }
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED,
                 "no fused kernel for gen " + std::to_string(a.gen) + " noise " + std::to_string(a.noise) +
                     " est " + std::to_string(a.est) + " model " + std::to_string(a.m->kind) + " payoff " +
@@ -371,7 +420,9 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     blocks = std::min<long long>(blocks, (long long)ki.blocks_per_sm * E.sm_count);
     blocks = std::max<long long>(blocks, 1);
     void* args[] = {&k};
+    if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[variant][0], ws.stream));
     MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kThreads), args, smem, ws.stream));
+    if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[variant][1], ws.stream));
     launch_finalize(k.partials, a.R, k.items_per_rep, nst, d_out, ws.stream);
     E.launches += 2;
     MCQ_CUDA(cudaGetLastError());

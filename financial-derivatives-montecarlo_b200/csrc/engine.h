@@ -75,6 +75,19 @@ struct KernelInfo {
     size_t smem = 0;
 };
 
+// Autotuner state of one kernel family with several compiled launch variants: the first two
+// large passes run one variant each, timed by events around the kernel on its own stream; the
+// variant with the lower time per path-step is kept.  Variants compute identical sums, so
+// tuning never changes a result.
+struct TuneState {
+    int chosen = -1;
+    bool done[2] = {false, false};
+    bool pending[2] = {false, false};
+    double per_unit[2] = {0.0, 0.0};
+    double units[2] = {0.0, 0.0};
+    cudaEvent_t ev[2][2] = {};
+};
+
 struct Engine {
     std::mutex mu;
     bool ready = false;
@@ -83,6 +96,7 @@ struct Engine {
     uint32_t* d_dv = nullptr;                        // JoeKuo6 table [20000][32]
     std::vector<std::unique_ptr<Workspace>> pool;    // pool[0] is the default workspace
     std::unordered_map<const void*, KernelInfo> kinfo;
+    std::unordered_map<uint64_t, TuneState> tune;
     int launches = 0;                                // kernel launches issued (accounting)
     Workspace& ws(int i);
 };

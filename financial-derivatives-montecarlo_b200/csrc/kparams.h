@@ -21,6 +21,7 @@ enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE
 constexpr int kWarpsPerBlock = 8;
 constexpr int kThreads = kWarpsPerBlock * 32;
 constexpr int kMaxBasket = 16;          // register-resident basket width
+constexpr int kMinBlocks = 3;           // resident CTAs per SM the register budget is set for
 constexpr int kMaxStats = 8;
 
 struct KParams {

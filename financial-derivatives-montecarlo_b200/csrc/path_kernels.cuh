@@ -65,8 +65,10 @@ __device__ __forceinline__ uint32_t hh_linear(uint32_t v, uint32_t base) {
 
 // u = ((float)s + 1) * 2^-32 as in methods_cuda.cu:823; u_cap is 1.0f in reference-compat
 // mode (u may be 1 -> +inf) and 1 - 2^-24 otherwise.
+// ((float)x + 1) * 2^-32 == fma((float)x, 2^-32, 2^-32) bit for bit: scaling by a power of two
+// is exact, so both round the same real number once.
 __device__ __forceinline__ float sobol_normal(uint32_t x, float u_cap) {
-    float u = ((float)x + 1.0f) * kTwoPow32Inv;
+    const float u = fmaf((float)x, kTwoPow32Inv, kTwoPow32Inv);
     return normcdfinvf(fminf(u, u_cap));
 }
 
@@ -214,14 +216,20 @@ __host__ __device__ constexpr bool path_dep() {
 // mu h per step that does not cancel between the fine and coarse paths of an MLMC level.)
 template <int MOD, int PAY>
 struct Leg {
-    float S, V, r0, r1;
+    // running accumulator: sums (Asian, geometric) keep a plain partial `tp` over at most 32
+    // steps that flush() folds into the Kahan pair (r0, r1); extrema live in r0
+    float S, V, r0, r1, tp;
+    static constexpr bool SUM = (PAY == PAY_ASIAN || PAY == PAY_GEOM);
     __device__ __forceinline__ void init(const KParams& p) {
-        S = p.S0; V = p.v0; r1 = 0.f;
+        S = p.S0; V = p.v0; r1 = 0.f; tp = 0.f;
         r0 = (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) ? p.S0 : 0.f;
     }
+    __device__ __forceinline__ void flush() {
+        if constexpr (SUM) { kadd(r0, r1, tp); tp = 0.f; }
+    }
     __device__ __forceinline__ void update() {
-        if constexpr (PAY == PAY_ASIAN) kadd(r0, r1, S);
-        else if constexpr (PAY == PAY_GEOM) kadd(r0, r1, logf(S));
+        if constexpr (PAY == PAY_ASIAN) tp += S;
+        else if constexpr (PAY == PAY_GEOM) tp += logf(S);
         else if constexpr (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) r0 = fminf(r0, S);
         else if constexpr (PAY == PAY_UPOUT) r0 = fmaxf(r0, S);
     }
@@ -242,6 +250,11 @@ struct Leg {
             V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
         }
         if constexpr (RUN && path_dep<PAY>()) update();
+    }
+    // GBM step from a raw normal: S + S (mu h + (sigma sqrt h) z)
+    __device__ __forceinline__ void step_gbm_z(float z, float sig_sqh, float muh) {
+        S = fmaf(S, fmaf(sig_sqh, z, muh), S);
+        if constexpr (path_dep<PAY>()) update();
     }
     __device__ __forceinline__ float payoff(const KParams& p, int n, float corr) const {
         if constexpr (PAY == PAY_EUR || PAY == PAY_BASKET) return fmaxf(S - p.K, 0.f) * p.disc;
@@ -292,20 +305,45 @@ struct PathC {
     }
     // raw normals, tile of 32 dimensions starting at a tile boundary
     __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
-        if constexpr (HES) {
+        if (nv == 32) {
+            if constexpr (HES) {
 #pragma unroll
-            for (int i = 0; i < 16; i++)
-                if (2 * i < nv) {
+                for (int i = 0; i < 16; i++) {
                     const float z1 = z[2 * i], z2 = z[2 * i + 1];
                     step_dw(p, z1 * p.sqrt_h, fmaf(p.L10, z1, p.L11 * z2) * p.sqrt_h);
                 }
-        } else {
+            } else if constexpr (MOD == MOD_GBM && !COUPLED) {
+                const float sig_sqh = p.sigma * p.sqrt_h;
 #pragma unroll
-            for (int i = 0; i < 32; i++)
-                if (i < nv) step_dw(p, z[i] * p.sqrt_h, 0.f);
+                for (int i = 0; i < 32; i++) f.step_gbm_z(z[i], sig_sqh, muh_f);
+                k += 32;
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; i++) step_dw(p, z[i] * p.sqrt_h, 0.f);
+            }
+        } else {
+            if constexpr (HES) {
+#pragma unroll
+                for (int i = 0; i < 16; i++)
+                    if (2 * i < nv) {
+                        const float z1 = z[2 * i], z2 = z[2 * i + 1];
+                        step_dw(p, z1 * p.sqrt_h, fmaf(p.L10, z1, p.L11 * z2) * p.sqrt_h);
+                    }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; i++)
+                    if (i < nv) step_dw(p, z[i] * p.sqrt_h, 0.f);
+            }
         }
+        flush();
+    }
+    // fold the running partial sums (called at least every 32 steps)
+    __device__ __forceinline__ void flush() {
+        f.flush();
+        if constexpr (COUPLED) c.flush();
     }
     __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        flush();
         const float pf = f.payoff(p, p.n_steps, p.corr_f);
         if constexpr (COUPLED) {
             const float pc = (p.n_coarse > 0) ? c.payoff(p, p.n_coarse, p.corr_c) : 0.f;
@@ -320,6 +358,7 @@ struct PathC {
 // Arithmetic Asian with geometric-Asian control on the same GBM path (kernel_gbm_asian_cv,
 // methods_cuda.cu:601-640): stats {Ya, Ya^2, Ycv, Ycv^2, Yg, Yg^2, Ya*Yg}.
 struct CvAsianC {
+    __device__ __forceinline__ void flush() {}
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr int NST = 7;
     float S, sa, ca, sl, cl, muh;
@@ -349,6 +388,7 @@ struct CvAsianC {
 // Dupire European with a GBM European control on the same increments
 // (kernel_dupire_gbm_cv, methods_cuda.cu:642-677).
 struct CvDupireC {
+    __device__ __forceinline__ void flush() {}
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr int NST = 7;
     float Sd, Sg, muh;
@@ -380,6 +420,7 @@ struct CvDupireC {
 // GBM European under the drift-shifted measure Z' = Z + z* with likelihood ratio
 // exp(-z* sum Z - N z*^2 / 2) (kernel_is_gbm, methods_cuda.cu:685-707).
 struct IsC {
+    __device__ __forceinline__ void flush() {}
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr int NST = 2;
     float S, zs, zc, muh;
@@ -409,6 +450,7 @@ struct IsC {
 template <int MOD, int NB>
 struct BasketC {
     static constexpr int NST = 2;
+    __device__ __forceinline__ void flush() {}
     __device__ __forceinline__ void bind(int, uint64_t) {}
     float S[NB], dw[NB];
     float muh;
@@ -474,6 +516,7 @@ struct BasketC {
 // Parity probe: records the normals (raw) or increments (bridge) the pass consumed for one
 // path, so tests can compare the fused generation bit for bit with the reference stream.
 struct DumpC {
+    __device__ __forceinline__ void flush() {}
     static constexpr int NST = 1;
     float* out;
     int idx;
@@ -523,6 +566,7 @@ __device__ __forceinline__ void bb_window(const KParams& p, C& cons, const float
     }
 #pragma unroll
     for (int t = 0; t < 32; t++) cons.step_dw(p, W[t + 1] - W[t], 0.f);
+    cons.flush();
 }
 
 // ------------------------------------------------------------------ the pass kernel
@@ -570,6 +614,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
 #pragma unroll
             for (int t = 0; t < 32; t++)
                 if (t < N) cons.step_dw(p, W[t + 1] - W[t], 0.f);
+            cons.flush();
         } else {
             // Skeleton W(32q), q = 0..S, from dimensions 0..S-1 (all multiples of 32), kept
             // per lane in shared memory at skel[q * 32 + lane]; then S windows of 32 steps.
@@ -611,8 +656,12 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
     }
 }
 
-template <int GEN, int NOISE, class C>
-__global__ void __launch_bounds__(kThreads, 2) k_pass(const __grid_constant__ KParams p) {
+// MINB: resident CTAs per SM the register budget is set for (0: 2 for the bridge, whose
+// window keeps 33 W values live, kMinBlocks otherwise).  Variants differ only in register
+// allocation and scheduling, never in arithmetic, so they produce identical sums.
+template <int GEN, int NOISE, class C, int MINB = 0>
+__global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ? 2 : kMinBlocks))
+    k_pass(const __grid_constant__ KParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int skel_floats = (NOISE == NOISE_BB && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;

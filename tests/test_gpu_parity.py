@@ -146,3 +146,17 @@ def test_cv_pilot_matches_pathwise_oracle(gpu, orc):
     cov = (ya * yg).mean() - ya.mean() * yg.mean()
     assert abs(got["var_plain"] - va) < 1e-4 * va
     assert abs(got["beta"] - np.clip(cov / vg, 0, 5)) < 1e-4
+
+
+@pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("heston", "lookback"), ("dupire", "eur")])
+def test_launch_variants_are_bit_identical(gpu, model, pay):
+    import os
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    out = []
+    try:
+        for v in ("0", "1"):
+            os.environ["MCQ_TUNE"] = v
+            out.append(gpu.qmc_pass(m, p, 64, salt_base=42, R=4, offset=3, n_points=50000))
+    finally:
+        os.environ.pop("MCQ_TUNE", None)
+    assert np.array_equal(out[0], out[1])
