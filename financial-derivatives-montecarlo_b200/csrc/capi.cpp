@@ -438,7 +438,10 @@ int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_han
     std::memset(&pay, 0, sizeof(pay));
     PassArgs a;
     a.m = m; a.p = &pay; a.n_steps = n_steps; a.gen = use_sobol ? GEN_SOBOL : GEN_PHILOX;
-    a.noise = noise_mode; a.bb = as_handle(bb, MCQ_NOISE_BB); a.seed = seed; a.salt0 = salt_base;
+    a.noise = noise_mode;
+    if (noise_mode == MCQ_NOISE_PCA) a.pca = as_handle(bb, MCQ_NOISE_PCA);
+    else a.bb = as_handle(bb, MCQ_NOISE_BB);
+    a.seed = seed; a.salt0 = salt_base;
     a.stream0 = salt_base; a.R = R; a.offset = offset; a.n_points = (uint64_t)n_points; a.flags = flags;
     a.dump = true;
     ensure_ready();

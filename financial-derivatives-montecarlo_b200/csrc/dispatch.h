@@ -10,6 +10,7 @@ const void* lookup_sobol_raw_plain(int model, int payoff);
 const void* lookup_sobol_raw_plain_b4(int model, int payoff);   // 64-register variant
 const void* lookup_sobol_raw_coupled(int model, int payoff);
 const void* lookup_sobol_bb(int model, int payoff, bool coupled);
+const void* lookup_sobol_pca_small(int model, int payoff, bool coupled);   // N <= 32
 const void* lookup_philox_plain(int model, int payoff);
 const void* lookup_philox_coupled(int model, int payoff);
 // est in {EST_CV_ASIAN, EST_CV_DUPIRE, EST_IS}, basket models (nb = 4, 8, 16), dump probes
@@ -32,6 +33,7 @@ inline const void* lookup_pass(int gen, int noise, int est, int model, int payof
     if (gen == GEN_SOBOL) {
         if (noise == NOISE_RAW) return cpl ? lookup_sobol_raw_coupled(model, payoff) : lookup_sobol_raw_plain(model, payoff);
         if (noise == NOISE_BB) return lookup_sobol_bb(model, payoff, cpl);
+        if (noise == NOISE_PCA) return lookup_sobol_pca_small(model, payoff, cpl);
         return nullptr;
     }
     if (noise != NOISE_RAW) return nullptr;

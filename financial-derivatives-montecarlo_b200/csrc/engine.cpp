@@ -10,6 +10,7 @@
 #include <cstring>
 
 #include "dispatch.h"
+#include "pca.h"
 #include "support.h"
 
 namespace mcq {
@@ -327,7 +328,20 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
         k.bb = (const float4*)a.bb->table.p;
         k.bbi = (const int2*)((const float4*)a.bb->table.p + a.n_steps);
     }
-    MCQ_REQUIRE(a.noise != NOISE_PCA, MCQ_ERR_UNSUPPORTED, "PCA pass not available in this build");
+    const bool pca_tc = (a.noise == NOISE_PCA) && D >= 64;
+    if (a.noise == NOISE_PCA) {
+        MCQ_REQUIRE(k.d_noise == 1, MCQ_ERR_UNSUPPORTED, "PCA needs a one-factor model");
+        MCQ_REQUIRE(a.gen == GEN_SOBOL, MCQ_ERR_UNSUPPORTED, "PCA is a QMC transform");
+        MCQ_REQUIRE(a.pca && a.pca->kind == MCQ_NOISE_PCA && a.pca->n == a.n_steps, MCQ_ERR_INVALID,
+                    "PCA handle missing or built for a different step count");
+        MCQ_REQUIRE(D <= 32 || D == 64 || D == 128 || D == 256, MCQ_ERR_UNSUPPORTED,
+                    "fused PCA supports N <= 32 and N in {64, 128, 256} steps; got " + std::to_string(D));
+        k.pca = a.pca->table.p;
+    }
+    if (pca_tc) {
+        pca_pass_async(ws, a, k, d_out);
+        return;
+    }
 
     const void* fn = a.dump ? lookup_misc(a.gen, a.noise, a.est, k.model, nb, true)
                             : lookup_pass(a.gen, a.noise, a.est, k.model, a.p->kind, nb);
@@ -428,6 +442,68 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     MCQ_CUDA(cudaGetLastError());
 }
 
+// Tensor-core PCA pass: CTA work items are runs of 256-path tiles of one replica; each item
+// leaves one record per warp, reduced per replica by k_finalize.
+void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out) {
+    Engine& E = engine();
+    const int N = k.D;
+    const void* fn = lookup_pca(k.model, a.p->kind, a.est == EST_COUPLED, a.dump);
+    MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no tensor-core PCA kernel for this model / payoff");
+    const uint64_t g0 = a.offset >> 5;
+    const uint64_t G = ((a.offset + a.n_points - 1) >> 5) - g0 + 1;
+    const uint64_t tiles = (G + 7) / 8;
+    const uint64_t target = 148ULL * 4;
+    uint64_t tpi = (tiles * (uint64_t)a.R + target - 1) / target;
+    if (tpi < 1) tpi = 1;
+    const uint64_t ipr = (tiles + tpi - 1) / tpi;
+    MCQ_REQUIRE(ipr * (uint64_t)a.R * pca_warps() < (1ull << 31), MCQ_ERR_RANGE, "too many work items");
+    k.R = a.R;
+    k.gpi = (int)tpi;
+    k.items_per_rep = (int)ipr;
+    k.n_items = (int)(ipr * a.R);
+    k.offset = a.offset;
+    k.n_points = a.n_points;
+    k.g0 = g0;
+    k.G = G;
+    if (!(ws.dirs_salt0 == a.salt0 && ws.dirs_R == a.R && ws.dirs_D == N)) {
+        uint32_t* d = (uint32_t*)ws.dirs.ensure(sizeof(uint32_t) * (size_t)a.R * 33 * N);
+        launch_prescramble(E.d_dv, a.salt0, a.R, N, d, ws.stream);
+        E.launches++;
+        ws.dirs_salt0 = a.salt0;
+        ws.dirs_R = a.R;
+        ws.dirs_D = N;
+    }
+    k.dirs = (const uint32_t*)ws.dirs.p;
+    const int nst = a.dump ? 1 : k.nstat;
+    k.nstat = nst;
+    k.partials = (double*)ws.partials.ensure(sizeof(double) * (size_t)k.n_items * pca_warps() * nst);
+    if (a.dump) k.dump = (float*)ws.dump.ensure(sizeof(float) * (size_t)a.R * a.n_points * N);
+    k.err = (int*)ws.err.ensure(sizeof(int));
+    MCQ_CUDA(cudaMemsetAsync(k.err, 0, sizeof(int), ws.stream));
+    ws.err_armed = true;
+    const size_t smem = pca_smem_bytes(N);
+    int per_sm = 0;
+    MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, pca_threads(), smem));
+    MCQ_REQUIRE(per_sm > 0, MCQ_ERR_INTERNAL, "PCA kernel does not fit on an SM");
+    long long blocks = std::min<long long>((long long)k.n_items, (long long)per_sm * E.sm_count);
+    blocks = std::max<long long>(blocks, 1);
+    void* args[] = {&k};
+    MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(pca_threads()), args, smem, ws.stream));
+    launch_finalize(k.partials, a.R, k.items_per_rep * pca_warps(), nst, d_out, ws.stream);
+    E.launches += 2;
+    MCQ_CUDA(cudaGetLastError());
+}
+
+// A bounded device wait that gave up leaves MCQ_ERR_TIMEOUT in the workspace's error word.
+static void check_err_word(Workspace& ws) {
+    if (!ws.err_armed) return;
+    int h = 0;
+    MCQ_CUDA(cudaMemcpy(&h, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    ws.err_armed = false;
+    MCQ_REQUIRE(h == 0, MCQ_ERR_TIMEOUT, "a bounded device-side wait timed out (status " + std::to_string(h) + ")");
+}
+
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a) {
     const size_t n = (size_t)a.R * (a.dump ? 1 : nstat_of(a.est));
     double* d = (double*)ws.sums.ensure(sizeof(double) * n);
@@ -435,6 +511,7 @@ std::vector<double> pass_sync(Workspace& ws, const PassArgs& a) {
     double* h = (double*)ws.hsums.ensure(sizeof(double) * n);
     MCQ_CUDA(cudaMemcpyAsync(h, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ws.stream));
     MCQ_CUDA(cudaStreamSynchronize(ws.stream));
+    check_err_word(ws);
     return std::vector<double>(h, h + n);
 }
 

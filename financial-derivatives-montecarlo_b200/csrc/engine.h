@@ -52,7 +52,8 @@ struct PinnedBuf {
 // small parameter uploads.  Launches on one workspace are ordered by its stream.
 struct Workspace {
     cudaStream_t stream = nullptr;
-    DevBuf partials, sums, dirs, aux, dump;
+    DevBuf partials, sums, dirs, aux, dump, err;
+    bool err_armed = false;   // err holds a fresh status from the last tensor-core pass
     PinnedBuf hsums, haux;
     uint32_t dirs_salt0 = 0;
     int dirs_R = -1, dirs_D = -1;
@@ -139,6 +140,8 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k);
 int nstat_of(int est);
 // Enqueue one pass on ws.stream; d_out receives [R][nstat] doubles (device).
 void pass_async(Workspace& ws, const PassArgs& a, double* d_out);
+// Tensor-core PCA pass (N in {64, 128, 256}); called by pass_async.
+void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out);
 // Enqueue, copy back and wait; returns [R][nstat].
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
 // Message returned by mcq_last_error() on this thread.

@@ -6,6 +6,7 @@ static const void* misc_gen(int noise, int est, int model, int nb, bool dump) {
     if (dump) {
         if (noise == NOISE_RAW) return (const void*)&k_pass<GEN, NOISE_RAW, DumpC>;
         if (noise == NOISE_BB && GEN == GEN_SOBOL) return (const void*)&k_pass<GEN_SOBOL, NOISE_BB, DumpC>;
+        if (noise == NOISE_PCA && GEN == GEN_SOBOL) return (const void*)&k_pass<GEN_SOBOL, NOISE_PCA, DumpC>;
         return nullptr;
     }
     if (noise != NOISE_RAW) return nullptr;

@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <type_traits>
+#include <cuda_fp16.h>
 #include "kparams.h"
 
 namespace mcq {
@@ -589,6 +590,26 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
             }
             cons.tile(p, z, min(32, D - d0));
         }
+    } else if constexpr (NOISE == NOISE_PCA) {
+        // N <= 32 (one tile): dW_i = sum_k M[i][k] z_k with z and M rounded to fp16 as the
+        // reference's cast + GEMM (methods_cuda.cu:1228-1229); larger N runs in k_pca.
+        const int N = D;
+        sobol_tile(dr, D, lane, lane < N, h, p.u_cap, buf, lane);
+        __syncwarp();
+        float z[32];
+        read_row(buf, lane, z);
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 32; j++) z[j] = __half2float(__float2half_rn(z[j]));
+        const __half* Mrow = static_cast<const __half*>(p.pca);
+        for (int i = 0; i < N; i++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                if (j < N) acc = fmaf(__half2float(Mrow[i * N + j]), z[j], acc);
+            cons.step_dw(p, acc, 0.f);
+        }
+        cons.flush();
     } else {   // NOISE_BB, one factor: D == n_steps == N (power of two)
         // Bridge table row j (Sobol dimension j = bb_precompute step j, utils.cpp:54-101):
         // p.bb[j] = {wl, wr, sd, bits(m)} and p.bbi[j] = {l, r}: W[m] = wl W[l] + wr W[r] + sd z_j.

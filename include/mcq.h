@@ -253,8 +253,9 @@ int mcq_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
 /* BB / PCA tables as the device sees them (for parity tests). */
 int mcq_bb_tables(mcq_handle bb, int* map_idx, float* wl, float* wr, float* sd);  /* per dimension */
 int mcq_pca_matrix(mcq_handle pca, float* M_colmajor_f32);
-/* The normals (raw) or time-ordered increments (bridge) that one fused pass consumed, for
-   bit-level parity tests: out_host[R][n_points][n_steps * d_noise].  n_points <= 2^20. */
+/* The normals (raw) or time-ordered increments (bridge, PCA) that one fused pass consumed,
+   for bit-level parity tests: out_host[R][n_points][n_steps * d_noise].  n_points <= 2^20.
+   `bb` is the BB handle for MCQ_NOISE_BB and the PCA handle for MCQ_NOISE_PCA. */
 int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_handle bb,
                         int use_sobol, uint32_t seed, uint32_t salt_base, int R, uint32_t offset,
                         int64_t n_points, int flags, float* out_host);

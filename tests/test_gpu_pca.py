@@ -1,0 +1,72 @@
+"""PCA ordering on the GPU: the tensor-core pass (tcgen05, N in {64, 128, 256}) and the
+single-tile pass (N <= 32) against an FP64 product on the same fp16-rounded inputs, the oracle,
+and the reference's own cuBLAS PCA pass (tests/golden)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def f16(x):
+    return np.asarray(x, np.float32).astype(np.float16).astype(np.float64)
+
+
+@pytest.mark.parametrize("N", [4, 32, 64, 128, 256])
+def test_pca_increments_match_fp64_product(gpu, N):
+    pca = gpu.pca_create(N, 1.0)
+    M = f16(gpu.pca_matrix(pca))                       # M[i, k] as the device sees it
+    R, n, off = 2, 300, 77
+    dump = gpu.debug_pass_dump(gpu.gbm(), N, gpu.PCA, bb=pca, use_sobol=True, salt_base=9, R=R, offset=off,
+                               n_points=n)
+    for r in range(R):
+        z = f16(gpu.sobol_hh_normal(9 + r, 0, N, off, n))   # [N, n]
+        ref = (M @ z).T                                      # [n, N]
+        assert np.allclose(dump[r], ref, atol=2e-6, rtol=2e-5), (r, np.abs(dump[r] - ref).max())
+    pca.close()
+
+
+@pytest.mark.parametrize("N", [32, 64, 256])
+@pytest.mark.parametrize("pay", ["asian", "eur", "lookback"])
+def test_pca_pass_vs_oracle(gpu, orc, N, pay):
+    m = gpu.gbm(100.0, 0.03, 0.25, 1.0)
+    p = {"asian": gpu.asian(100.0), "eur": gpu.european(100.0, 0.03, 1.0), "lookback": gpu.lookback(0.25)}[pay]
+    pca = gpu.pca_create(N, 1.0)
+    R, Np = 2, 2048
+    g = gpu.qmc_pass(m, p, N, noise=gpu.PCA, pca=pca, salt_base=42, R=R, offset=0, n_points=Np)
+    o = orc.qmc_sums(m, p, N, orc.noise(orc.T.PCA, N, 1.0), salt_base=42, R=R, offset=0, N=Np)
+    for r in range(R):
+        assert abs(g[r, 0] / Np - o[r, 0] / Np) < 3e-4 * (1 + abs(o[r, 0] / Np)), (r, g[r], o[r])
+    pca.close()
+
+
+def test_pca_pass_equals_reference_cublas_pass(gpu):
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import golden_cases
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_golden.npz"))
+    case = {c[0]: c for c in golden_cases.cases(gpu.mcq_types)}["asian_pca_256"]
+    _, m, p, n_steps, mode, salt0, R, off, N = case
+    pca = gpu.pca_create(n_steps, 1.0)
+    mine = gpu.qmc_pass(m, p, n_steps, noise=gpu.PCA, pca=pca, salt_base=salt0, R=R, offset=off, n_points=N)
+    ref = gold["pass_asian_pca_256"]
+    for r in range(R):
+        assert abs(mine[r, 0] / N - ref[r, 0] / N) < 1e-4 * (1 + abs(ref[r, 0] / N)), (r, mine[r], ref[r])
+    pca.close()
+
+
+def test_pca_qmc_driver_and_mlqmc(gpu, orc):
+    m, p = gpu.gbm(100.0, 0.03, 0.25, 1.0), gpu.asian(100.0)
+    pca = gpu.pca_create(256, 1.0)
+    r = gpu.run_qmc(m, p, 2e-3, 256, gpu.qmc_cfg(R=32, N0_per_replica=1 << 12), noise=gpu.PCA, pca=pca)
+    raw = gpu.run_qmc(m, p, 2e-3, 256, gpu.qmc_cfg(R=32, N0_per_replica=1 << 12))
+    assert abs(r["price"] - raw["price"]) < 4 * np.hypot(r["std_error"], raw["std_error"]), (r, raw)
+    pca.close()
+    me, pe = gpu.gbm(100, 0.05, 0.2, 1.0), gpu.european(100, 0.05, 1.0)
+    lst = [gpu.pca_create(1 << l, 1.0) for l in range(9)]
+    q = gpu.run_mlqmc(me, pe, 5e-3, gpu.mlmc_cfg(max_L=8), gpu.qmc_cfg(R=16), noise=gpu.PCA, pca_list=lst)
+    bs = orc.bs_call(100, 100, 1, 0.05, 0.2)
+    assert abs(q["price"] - bs) < 4 * q["std_error"] + 5e-3 / np.sqrt(2), q
+    for h in lst:
+        h.close()
