@@ -164,6 +164,7 @@ def main():
     ap.add_argument("--points", type=int, default=1 << 20, help="points per replica per step")
     ap.add_argument("--e2e-runs", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true", help="skip the bridge / PCA orderings")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -223,6 +224,30 @@ def main():
     chk = sums.cpu().numpy().reshape(REPS, 2)
     price = float((chk[:, 0] / N).mean())
 
+    # the same workload under Brownian-bridge and PCA (tcgen05) ordering, same timing rules
+    variants = {}
+    if not args.no_variants:
+        for name, noise in (("bridge", eng.BB), ("pca_tcgen05", eng.PCA)):
+            h = eng.bb_create(STEPS, T_) if noise == eng.BB else eng.pca_create(STEPS, T_)
+            kw = {"bb": h} if noise == eng.BB else {"pca": h}
+            for _ in range(args.warmup):
+                eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, noise=noise, salt_base=salt, R=REPS,
+                                    n_points=N, **kw)
+            tv = 0.0
+            for i in range(max(3, args.steps // 2)):
+                flush.zero_()
+                a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a_.record(stream)
+                eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, noise=noise, salt_base=salt, R=REPS,
+                                    n_points=N, **kw)
+                b_.record(stream)
+                b_.synchronize()
+                tv += a_.elapsed_time(b_)
+            nv = max(3, args.steps // 2)
+            variants[name] = {"value": ps_per_step * nv / (tv * 1e-3), "ms_per_step": tv / nv,
+                              "price": float((sums.cpu().numpy().reshape(REPS, 2)[:, 0] / N).mean())}
+            h.close()
+
     # e2e: the reference-facing adaptive driver with host structs
     cfg = eng.qmc_cfg(R=REPS, N0_per_replica=1 << 14, salt_base=salt)
     eng.run_qmc(m, p, 1e-3, STEPS, cfg)   # warm-up (tables, streams)
@@ -256,10 +281,9 @@ def main():
     per_launch_ms = total_ms / args.steps
     achieved = ps_per_step * FLOPS_PER_PATH_STEP / (per_launch_ms * 1e-3) / 1e12
     traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            tj = json.load(f)
-        traffic = tj["bytes_per_path_step"] * ps_per_step
+    try:   # DRAM bytes of one launch from the committed ncu capture (independent of the path count)
+        with open(os.path.join(ROOT, "profiles", "traffic_k_pass.json")) as f:
+            traffic = json.load(f)["dram_bytes_per_launch"]
     except (OSError, ValueError, KeyError):
         pass
     line = {
@@ -272,6 +296,7 @@ def main():
                    "seq_len": STEPS, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed (256 MiB write) between steps; inputs are parameter-sized"},
         "price_check": price,
+        "orderings": variants,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": doublings * REPS * 2 * 8,
                 "what": "mcq_run_qmc (run_qmc_cuda entry) eps=1e-3 from 2^14 pts/replica, host wall time; "

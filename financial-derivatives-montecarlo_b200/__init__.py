@@ -13,7 +13,7 @@ from .mcq_types import (  # noqa: F401  (re-exported builders)
     GBM, HESTON, DUPIRE, MULTI_DUPIRE, LOCALVOL_GRID, BASKET_GBM,
     EUROPEAN, ASIAN, GEOM_ASIAN, LOOKBACK, BARRIER_UP_OUT, BASKET, BARRIER_DOWN_OUT,
     RAW, BB, PCA, FLAG_COMPAT_U_INF, FLAG_COMPAT_HESTON_MLMC,
-    gbm, heston, dupire, multi_dupire, basket_gbm, localvol_grid, payoff, european, asian,
+    gbm, heston, dupire, multi_dupire, basket_gbm, localvol_grid, config4_surface, payoff, european, asian,
     geom_asian, lookback, barrier_up_out, barrier_down_out, basket, noise_dim,
 )
 
@@ -26,7 +26,7 @@ EXPORTS = [
     "mcq_run_mc", "mcq_run_mc_fixed", "mcq_run_qmc", "mcq_run_mlmc", "mcq_run_mlqmc", "mcq_cv_pilot",
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
     "mcq_mc_pass", "mcq_level_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
-    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_qmc_pass_noalloc",
+    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_qmc_pass_noalloc", "mcq_adjoint",
 ]
 
 
@@ -237,6 +237,19 @@ def qmc_pass_noalloc(m, p, n_steps, sums_device_ptr, stream_ptr=0, salt_base=42,
     _check(lib().mcq_qmc_pass_noalloc(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_uint32(salt_base), C.c_int(R),
                                       C.c_uint32(offset), C.c_int64(n_points), C.c_int(flags),
                                       C.c_void_p(sums_device_ptr), C.c_void_p(stream_ptr)))
+
+
+def adjoint(m, p, n_steps, salt_base=42, R=16, offset=0, n_points=4096, flags=0):
+    """mcq_adjoint: pathwise Greeks; returns (dict, node_vega array or None)."""
+    g = T.Greeks()
+    nodes = np.zeros(m.lv_nK * m.lv_nt, np.float64) if m.kind == LOCALVOL_GRID else None
+    _check(lib().mcq_adjoint(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_uint32(salt_base), C.c_int(R),
+                             C.c_uint32(offset), C.c_int64(n_points), C.c_int(flags), C.byref(g),
+                             nodes.ctypes.data_as(_P(C.c_double)) if nodes is not None else None))
+    d = {k: getattr(g, k) for k, _ in g._fields_}
+    if nodes is not None:
+        nodes = nodes.reshape(m.lv_nt, m.lv_nK)
+    return d, nodes
 
 
 def mc_pass(m, p, n_steps, seed, stream_id, first_path, n_paths):

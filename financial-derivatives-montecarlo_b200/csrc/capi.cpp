@@ -452,6 +452,18 @@ int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_han
     API_END
 }
 
+// ------------------------------------------------------------------ adjoint Greeks
+
+int mcq_adjoint(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t salt_base, int R,
+                uint32_t offset, int64_t n_points, int flags, mcq_greeks* out, double* node_vega) {
+    API_BEGIN
+    NEED(m); NEED(p); NEED(out);
+    MCQ_REQUIRE(n_points >= 1 && R >= 1, MCQ_ERR_INVALID, "bad R / n_points");
+    ensure_ready();
+    adjoint_run(*m, *p, n_steps, salt_base, R, offset, (uint64_t)n_points, flags, *out, node_vega);
+    API_END
+}
+
 // ------------------------------------------------------------------ parity exports
 
 static void sobol_export(uint32_t salt, int dim0, int nd, uint32_t offset, int64_t n, int flags,

@@ -6,9 +6,11 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 
+#include "adjoint.h"
 #include "dispatch.h"
 #include "pca.h"
 #include "support.h"
@@ -211,6 +213,7 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
 
     k.K = (float)p.K;
     k.B = (float)p.B;
+    k.pay_T = (float)p.T;
     switch (p.kind) {
         case MCQ_PAYOFF_EUROPEAN:
         case MCQ_PAYOFF_BARRIER_UP_OUT:
@@ -238,8 +241,8 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
     if (m.kind == MCQ_MODEL_MULTI_DUPIRE || m.kind == MCQ_MODEL_BASKET_GBM) {
         const int n = m.n_assets;
         MCQ_REQUIRE(n >= 1, MCQ_ERR_INVALID, "basket needs n_assets >= 1");
-        MCQ_REQUIRE(n <= kMaxBasket, MCQ_ERR_UNSUPPORTED,
-                    "basket width " + std::to_string(n) + " exceeds the register-resident limit 16");
+        MCQ_REQUIRE(n <= 128, MCQ_ERR_UNSUPPORTED,
+                    "basket width " + std::to_string(n) + " exceeds the limit of 128 assets");
         MCQ_REQUIRE(m.S0_vec != nullptr, MCQ_ERR_INVALID, "basket needs S0_vec");
         if (m.kind == MCQ_MODEL_BASKET_GBM)
             MCQ_REQUIRE(m.sigma_vec != nullptr, MCQ_ERR_INVALID, "basket needs sigma_vec");
@@ -284,7 +287,7 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
 // ------------------------------------------------------------------ launcher
 
 
-static KernelInfo& kernel_info(const void* fn, size_t smem) {
+KernelInfo& kernel_info(const void* fn, size_t smem) {
     Engine& E = engine();
     auto it = E.kinfo.find(fn);
     if (it != E.kinfo.end() && it->second.smem == smem) return it->second;
@@ -513,6 +516,96 @@ std::vector<double> pass_sync(Workspace& ws, const PassArgs& a) {
     MCQ_CUDA(cudaStreamSynchronize(ws.stream));
     check_err_word(ws);
     return std::vector<double>(h, h + n);
+}
+
+}  // namespace mcq
+
+namespace mcq {
+
+// ------------------------------------------------------------------ adjoint Greeks
+
+void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t salt_base, int R,
+                 uint64_t offset, uint64_t n_points, int flags, mcq_greeks& out, double* node_vega) {
+    Engine& E = engine();
+    MCQ_REQUIRE(m.kind == MCQ_MODEL_GBM || m.kind == MCQ_MODEL_DUPIRE || m.kind == MCQ_MODEL_LOCALVOL_GRID,
+                MCQ_ERR_UNSUPPORTED, "adjoint Greeks: GBM, parametric Dupire or grid local-vol models");
+    MCQ_REQUIRE(p.kind == MCQ_PAYOFF_EUROPEAN || p.kind == MCQ_PAYOFF_ASIAN || p.kind == MCQ_PAYOFF_LOOKBACK,
+                MCQ_ERR_UNSUPPORTED, "adjoint Greeks: European, Asian or lookback payoffs (Lipschitz)");
+    MCQ_REQUIRE(n_steps >= 32 && n_steps % 32 == 0 && n_steps <= 1024, MCQ_ERR_UNSUPPORTED,
+                "adjoint Greeks: n_steps must be a multiple of 32 in [32, 1024]");
+    MCQ_REQUIRE(R >= 1 && n_points >= 1 && offset + n_points <= (1ull << 32), MCQ_ERR_RANGE, "bad replica / point range");
+    auto t0 = std::chrono::steady_clock::now();
+    const int l0 = E.launches;
+    Workspace& ws = E.ws(0);
+    PassArgs a;
+    a.m = &m; a.p = &p; a.n_steps = n_steps; a.gen = GEN_SOBOL; a.salt0 = salt_base; a.R = R;
+    a.offset = offset; a.n_points = n_points; a.flags = flags;
+    KParams k;
+    fill_params(ws, a, k);
+    const int n_nodes = (m.kind == MCQ_MODEL_LOCALVOL_GRID) ? m.lv_nK * m.lv_nt : 0;
+    MCQ_REQUIRE(n_nodes <= 4096, MCQ_ERR_UNSUPPORTED, "adjoint Greeks: at most 4096 grid nodes");
+    const void* fn = lookup_adjoint(k.model, p.kind);
+    MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no adjoint kernel for this model / payoff");
+    const uint64_t g0 = offset >> 5;
+    const uint64_t G = ((offset + n_points - 1) >> 5) - g0 + 1;
+    const long long target = kTargetItems / 2;
+    uint64_t gpi = (G * (uint64_t)R + target - 1) / target;
+    if (gpi < 1) gpi = 1;
+    const uint64_t ipr = (G + gpi - 1) / gpi;
+    k.R = R; k.gpi = (int)gpi; k.items_per_rep = (int)ipr; k.n_items = (int)(ipr * R);
+    k.offset = offset; k.n_points = n_points; k.g0 = g0; k.G = G;
+    if (!(ws.dirs_salt0 == salt_base && ws.dirs_R == R && ws.dirs_D == n_steps)) {
+        uint32_t* d = (uint32_t*)ws.dirs.ensure(sizeof(uint32_t) * (size_t)R * 33 * n_steps);
+        launch_prescramble(E.d_dv, salt_base, R, n_steps, d, ws.stream);
+        E.launches++;
+        ws.dirs_salt0 = salt_base; ws.dirs_R = R; ws.dirs_D = n_steps;
+    }
+    k.dirs = (const uint32_t*)ws.dirs.p;
+    k.nstat = 4;
+    k.partials = (double*)ws.partials.ensure(sizeof(double) * (size_t)k.n_items * 4);
+    double* d_nodes = nullptr;
+    if (n_nodes) {
+        d_nodes = (double*)ws.dump.ensure(sizeof(double) * n_nodes);
+        MCQ_CUDA(cudaMemsetAsync(d_nodes, 0, sizeof(double) * n_nodes, ws.stream));
+    }
+    k.node_out = d_nodes;
+    const size_t smem = adjoint_smem_bytes(n_steps, n_nodes);
+    KernelInfo& ki = kernel_info(fn, smem);
+    long long blocks = std::min<long long>(((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock,
+                                           (long long)ki.blocks_per_sm * E.sm_count);
+    blocks = std::max<long long>(blocks, 1);
+    double* d_out = (double*)ws.sums.ensure(sizeof(double) * (size_t)R * 4);
+    void* args[] = {&k};
+    MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kThreads), args, smem, ws.stream));
+    launch_finalize(k.partials, R, k.items_per_rep, 4, d_out, ws.stream);
+    E.launches += 2;
+    MCQ_CUDA(cudaGetLastError());
+    std::vector<double> s((size_t)R * 4);
+    MCQ_CUDA(cudaMemcpyAsync(s.data(), d_out, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, ws.stream));
+    std::vector<double> nv(n_nodes);
+    if (n_nodes)
+        MCQ_CUDA(cudaMemcpyAsync(nv.data(), d_nodes, sizeof(double) * n_nodes, cudaMemcpyDeviceToHost, ws.stream));
+    MCQ_CUDA(cudaStreamSynchronize(ws.stream));
+    double mean[4] = {0, 0, 0, 0}, se[4] = {0, 0, 0, 0};
+    for (int q = 0; q < 4; q++) {
+        for (int r = 0; r < R; r++) mean[q] += s[4 * r + q] / (double)n_points;
+        mean[q] /= R;
+        double v = 0;
+        for (int r = 0; r < R; r++) {
+            const double d = s[4 * r + q] / (double)n_points - mean[q];
+            v += d * d;
+        }
+        se[q] = R > 1 ? std::sqrt(v / (R - 1) / R) : 0.0;
+    }
+    out.price = mean[0]; out.delta = mean[1]; out.rho = mean[2]; out.vega = mean[3];
+    out.price_se = se[0]; out.delta_se = se[1]; out.rho_se = se[2]; out.vega_se = se[3];
+    out.n_paths = (int64_t)R * (int64_t)n_points;
+    out.n_nodes = n_nodes;
+    out.launches = E.launches - l0;
+    out.path_steps = 3.0 * (double)out.n_paths * n_steps;   // forward + recompute + reverse
+    if (node_vega)
+        for (int i = 0; i < n_nodes; i++) node_vega[i] = nv[i] / (double)out.n_paths;
+    out.time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 }  // namespace mcq

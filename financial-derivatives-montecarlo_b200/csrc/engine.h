@@ -144,6 +144,11 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out);
 void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out);
 // Enqueue, copy back and wait; returns [R][nstat].
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
+// Occupancy / shared-memory set-up of a kernel for a dynamic shared-memory size (cached).
+KernelInfo& kernel_info(const void* fn, size_t smem);
+// Pathwise adjoint Greeks over R scrambled replicas (k_adjoint.cu).
+void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t salt_base, int R,
+                 uint64_t offset, uint64_t n_points, int flags, mcq_greeks& out, double* node_vega);
 // Message returned by mcq_last_error() on this thread.
 void set_last_error(const std::string& msg);
 // Device capacity used by the reference's memory-derived batch sizing.

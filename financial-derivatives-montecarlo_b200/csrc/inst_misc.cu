@@ -17,12 +17,14 @@ static const void* misc_gen(int noise, int est, int model, int nb, bool dump) {
         if (nb <= 4) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_MULTI, 4>>;
         if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_MULTI, 8>>;
         if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_MULTI, 16>>;
+        if (nb <= kMaxWideBasket) return (const void*)&k_pass<GEN, NOISE_RAW, BasketWideC<MOD_MULTI>>;
         return nullptr;
     }
     if (model == MOD_BASKET) {
         if (nb <= 4) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_BASKET, 4>>;
         if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_BASKET, 8>>;
         if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_BASKET, 16>>;
+        if (nb <= kMaxWideBasket) return (const void*)&k_pass<GEN, NOISE_RAW, BasketWideC<MOD_BASKET>>;
         return nullptr;
     }
     return nullptr;

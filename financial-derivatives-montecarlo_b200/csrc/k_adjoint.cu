@@ -1,0 +1,231 @@
+// k_adjoint.cu — pathwise adjoint Greeks on scrambled-Sobol paths (no counterpart in the
+// reference, which computes no sensitivities).
+//
+// For each path (lane) the forward sweep steps S_k -> S_{k+1} = S_k (1 + mu h + sigma_k dW_k),
+// keeps the payoff state and checkpoints S every 16 steps in shared memory.  The reverse sweep
+// walks the 32-step Sobol tiles backwards: it regenerates the tile's normals (same warp-
+// transposed generator as the pricing pass), recomputes each 16-step segment from its
+// checkpoint, and propagates
+//     Sbar_k = Sbar_{k+1} dS_{k+1}/dS_k + dP/dS_k,
+//     mubar += Sbar_{k+1} S_k h,            sigmabar += Sbar_{k+1} dS_{k+1}/dsigma,
+// and, for the grid local-vol model, adds Sbar_{k+1} S_k dW_k w_n to the four bilinear nodes n of
+// (S_k, t_k) in an FP64 shared-memory array per CTA.  Payoffs are the Lipschitz ones:
+// European (discounted), arithmetic Asian and floating-strike lookback (BGK factor constant).
+// Per path it yields P, delta = Sbar_0, rho = mubar (+ -T P for the discounted European, the
+// drift and the discount sharing the rate) and vega (GBM: d/dsigma; Dupire: d/dsigma0; grid:
+// the parallel shift = sum of node vegas).
+#include "adjoint.h"
+#include "path_kernels.cuh"
+
+namespace mcq {
+
+constexpr int kCk = 16;   // checkpoint interval (steps)
+
+struct LvEval {
+    float sig, dsig;
+    int n00;              // node index (j * nK + i) of the lower-left corner
+    float w00, w01, w10, w11;
+};
+
+// bilinear sigma(S, t) on the uniform grid exactly as lv_sigma, with dsigma/dS and the weights
+__device__ __forceinline__ LvEval lv_eval(const KParams& p, float S, float t) {
+    LvEval e;
+    float x = (S - p.lv_K0) * p.lv_inv_dK;
+    const bool inside = x > 0.f && x < (float)(p.lv_nK - 1);
+    x = fminf(fmaxf(x, 0.f), (float)(p.lv_nK - 1));
+    const int i = min((int)x, p.lv_nK - 2);
+    const float a = x - (float)i;
+    float y = (t - p.lv_t0) * p.lv_inv_dt;
+    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
+    const int j = min((int)y, p.lv_nt - 2);
+    const float b = y - (float)j;
+    const float* g = p.lv + j * p.lv_nK + i;
+    const float s00 = __ldg(g), s01 = __ldg(g + 1), s10 = __ldg(g + p.lv_nK), s11 = __ldg(g + p.lv_nK + 1);
+    const float lo = fmaf(a, s01 - s00, s00), hi = fmaf(a, s11 - s10, s10);
+    e.sig = fmaf(b, hi - lo, lo);
+    e.dsig = inside ? ((1.f - b) * (s01 - s00) + b * (s11 - s10)) * p.lv_inv_dK : 0.f;
+    e.n00 = j * p.lv_nK + i;
+    e.w00 = (1.f - a) * (1.f - b);
+    e.w01 = a * (1.f - b);
+    e.w10 = (1.f - a) * b;
+    e.w11 = a * b;
+    return e;
+}
+
+// local volatility and its S-derivative / sigma-parameter derivative for the model
+template <int MOD>
+__device__ __forceinline__ float local_sigma(const KParams& p, float S, float t, float* dsig_dS,
+                                             float* dsig_dpar, LvEval* lv) {
+    if constexpr (MOD == MOD_GBM) {
+        *dsig_dS = 0.f;
+        *dsig_dpar = 1.f;
+        return p.sigma;
+    } else if constexpr (MOD == MOD_DUPIRE) {
+        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S * p.inv_S0), -p.alpha * t * kLog2e));
+        *dsig_dS = sl * p.bm1 / S;
+        *dsig_dpar = sl / p.sigma0;
+        return sl;
+    } else {
+        *lv = lv_eval(p, S, t);
+        *dsig_dS = lv->dsig;
+        *dsig_dpar = 1.f;
+        return lv->sig;
+    }
+}
+
+template <int MOD, int PAY>
+__global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__ KParams p) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int N = p.n_steps;
+    const int n_ck = N / kCk + 1;
+    const int per_warp = 1024 + n_ck * 32 + kCk * 32;
+    double* nodes = reinterpret_cast<double*>(smem4);             // [n_nodes] FP64, CTA-wide
+    const int node_doubles = (MOD == MOD_LVGRID) ? ((p.lv_nK * p.lv_nt + 1) & ~1) : 0;
+    float* wbase = reinterpret_cast<float*>(nodes + node_doubles) + wib * per_warp;
+    float* buf = wbase;               // 32 x 32 transpose tile
+    float* ck = wbase + 1024;         // checkpoints [n_ck][32]
+    float* seg = ck + n_ck * 32;      // recomputed segment [16][32]
+    if constexpr (MOD == MOD_LVGRID) {
+        for (int i = threadIdx.x; i < node_doubles; i += blockDim.x) nodes[i] = 0.0;
+        __syncthreads();
+    }
+    const float h = p.h, sqh = p.sqrt_h, muh = p.mu * p.h;
+    const int total_warps = gridDim.x * kWarpsPerBlock;
+    const uint64_t gend_all = p.g0 + p.G;
+    for (int item = blockIdx.x * kWarpsPerBlock + wib; item < p.n_items; item += total_warps) {
+        const int r = item / p.items_per_rep;
+        const int j = item - r * p.items_per_rep;
+        const uint64_t gb = p.g0 + (uint64_t)j * (uint64_t)p.gpi;
+        const uint64_t ge = min(gb + (uint64_t)p.gpi, gend_all);
+        const uint32_t* dr = p.dirs + (size_t)r * 33 * (size_t)N;
+        Acc<4> acc;
+        acc.zero();
+        for (uint64_t hg = gb; hg < ge; hg++) {
+            const uint64_t n = hg * 32 + (uint64_t)lane;
+            const bool valid = n >= p.offset && n < p.offset + p.n_points;
+            // ---------------- forward sweep
+            float S = p.S0, ts = 0.f, tot = 0.f, comp = 0.f, mn = p.S0;
+            int kmin = 0;
+            for (int d0 = 0; d0 < N; d0 += 32) {
+                sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 32; i++) {
+                    const int k = d0 + i;
+                    if ((i & (kCk - 1)) == 0) ck[(k / kCk) * 32 + lane] = S;
+                    float dsS, dsP;
+                    LvEval lv;
+                    const float sig = local_sigma<MOD>(p, S, (float)k * h, &dsS, &dsP, &lv);
+                    S = fmaf(S, fmaf(sig, z[i] * sqh, muh), S);
+                    if constexpr (PAY == PAY_ASIAN) ts += S;
+                    if constexpr (PAY == PAY_LOOKBACK) {
+                        if (S < mn) { mn = S; kmin = k + 1; }
+                    }
+                }
+                if constexpr (PAY == PAY_ASIAN) { kadd(tot, comp, ts); ts = 0.f; }
+            }
+            // payoff and its direct derivatives
+            float P, g_all = 0.f, Sbar;
+            if constexpr (PAY == PAY_EUR) {
+                P = fmaxf(S - p.K, 0.f) * p.disc;
+                Sbar = (S > p.K) ? p.disc : 0.f;
+            } else if constexpr (PAY == PAY_ASIAN) {
+                const float A = (tot - comp) / (float)N;
+                P = fmaxf(A - p.K, 0.f);
+                g_all = (A > p.K) ? 1.f / (float)N : 0.f;
+                Sbar = g_all;
+            } else {   // floating-strike lookback
+                P = S - mn * p.corr_f;
+                Sbar = 1.f + ((kmin == N) ? -p.corr_f : 0.f);
+            }
+            // ---------------- reverse sweep
+            float mubar = 0.f, sigbar = 0.f;
+            for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
+                sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+#pragma unroll
+                for (int s = 1; s >= 0; s--) {
+                    const int k0 = d0 + s * kCk;
+                    float Sr = ck[(k0 / kCk) * 32 + lane];
+#pragma unroll
+                    for (int i = 0; i < kCk; i++) {
+                        seg[i * 32 + lane] = Sr;
+                        float dsS, dsP;
+                        LvEval lv;
+                        const float sig = local_sigma<MOD>(p, Sr, (float)(k0 + i) * h, &dsS, &dsP, &lv);
+                        Sr = fmaf(Sr, fmaf(sig, z[s * kCk + i] * sqh, muh), Sr);
+                    }
+#pragma unroll
+                    for (int i = kCk - 1; i >= 0; i--) {
+                        const int k = k0 + i;
+                        const float Sk = seg[i * 32 + lane];
+                        const float dw = z[s * kCk + i] * sqh;
+                        float dsS, dsP;
+                        LvEval lv;
+                        const float sig = local_sigma<MOD>(p, Sk, (float)k * h, &dsS, &dsP, &lv);
+                        mubar = fmaf(Sbar, Sk * h, mubar);
+                        const float sens = Sbar * Sk * dw;     // dP/dsigma_k through this step
+                        sigbar = fmaf(sens, dsP, sigbar);
+                        if constexpr (MOD == MOD_LVGRID) {
+                            if (valid && sens != 0.f) {
+                                atomicAdd(&nodes[lv.n00], (double)(sens * lv.w00));
+                                atomicAdd(&nodes[lv.n00 + 1], (double)(sens * lv.w01));
+                                atomicAdd(&nodes[lv.n00 + p.lv_nK], (double)(sens * lv.w10));
+                                atomicAdd(&nodes[lv.n00 + p.lv_nK + 1], (double)(sens * lv.w11));
+                            }
+                        }
+                        const float dS1 = 1.f + muh + sig * dw + Sk * dw * dsS;
+                        float direct = 0.f;
+                        if constexpr (PAY == PAY_ASIAN) direct = (k >= 1) ? g_all : 0.f;
+                        if constexpr (PAY == PAY_LOOKBACK) direct = (k == kmin) ? -p.corr_f : 0.f;
+                        Sbar = fmaf(Sbar, dS1, direct);
+                    }
+                }
+            }
+            float rho = mubar;
+            if constexpr (PAY == PAY_EUR) rho -= p.pay_T * P;
+            float y[4] = {P, Sbar, rho, sigbar};
+            if (valid) acc.add(y);
+        }
+        acc.flush(p.partials + (size_t)item * 4, lane);
+    }
+    if constexpr (MOD == MOD_LVGRID) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < p.lv_nK * p.lv_nt; i += blockDim.x)
+            if (nodes[i] != 0.0) atomicAdd(p.node_out + i, nodes[i]);
+    }
+}
+
+template <int MOD>
+static const void* adj_payoff(int pay) {
+    switch (pay) {
+        case PAY_EUR: return (const void*)&k_adjoint<MOD, PAY_EUR>;
+        case PAY_ASIAN: return (const void*)&k_adjoint<MOD, PAY_ASIAN>;
+        case PAY_LOOKBACK: return (const void*)&k_adjoint<MOD, PAY_LOOKBACK>;
+        default: return nullptr;
+    }
+}
+
+const void* lookup_adjoint(int model, int payoff) {
+    switch (model) {
+        case MOD_GBM: return adj_payoff<MOD_GBM>(payoff);
+        case MOD_DUPIRE: return adj_payoff<MOD_DUPIRE>(payoff);
+        case MOD_LVGRID: return adj_payoff<MOD_LVGRID>(payoff);
+        default: return nullptr;
+    }
+}
+
+size_t adjoint_smem_bytes(int n_steps, int n_nodes) {
+    const int n_ck = n_steps / kCk + 1;
+    const size_t per_warp = (size_t)(1024 + n_ck * 32 + kCk * 32) * sizeof(float);
+    return (size_t)((n_nodes + 1) & ~1) * sizeof(double) + kWarpsPerBlock * per_warp;
+}
+
+}  // namespace mcq

@@ -50,6 +50,7 @@ struct KParams {
     float hc, em_c;                                // coarse step, exp(-kappa hc)
     // ---- payoff
     float K, B, disc, corr_f, corr_c, u_cap;
+    float pay_T;                                   // payoff maturity (discount sensitivity)
     // ---- control variate / importance sampling
     float beta_cv, E_ctrl, z_star;
     float ctrl_sigma;                              // GBM control volatility (EST_CV_DUPIRE)
@@ -76,6 +77,8 @@ struct KParams {
     double* partials;
     // ---- parity dump (DumpC only): [R][n_points][D] normals (raw) or increments (bridge)
     float* dump;
+    // ---- adjoint: per-node local-vol sensitivities, summed over paths (FP64)
+    double* node_out;
     // ---- bounded-wait / error reporting
     int* err;
 };

@@ -540,6 +540,71 @@ struct DumpC {
     __device__ __forceinline__ void finish(const KParams&, float (&y)[NST]) { y[0] = 0.f; }
 };
 
+// Wide basket (up to kMaxWideBasket assets, e.g. the reference's 100-asset example): the same
+// arithmetic as BasketC with the per-asset state in local memory and rolled loops.
+constexpr int kMaxWideBasket = 128;
+template <int MOD>
+struct BasketWideC {
+    static constexpr int NST = 2;
+    float S[kMaxWideBasket], dw[kMaxWideBasket];
+    float muh;
+    int f, k;
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    __device__ __forceinline__ void flush() {}
+    __device__ __forceinline__ void init(const KParams& p) {
+        const int n = p.n_assets;
+#pragma unroll 1
+        for (int a = 0; a < n; a++) { S[a] = __ldg(p.bsk + a); dw[a] = 0.f; }
+        muh = p.mu * p.h;
+        f = 0; k = 0;
+    }
+    __device__ __forceinline__ void feed(const KParams& p, float z) {
+        const int n = p.n_assets;
+        const float x = z * p.sqrt_h;
+        if (p.uncorrelated) {
+            dw[f] = x;
+        } else {
+            const float* Lcol = p.bsk + 3 * n + f;
+#pragma unroll 1
+            for (int a = f; a < n; a++) dw[a] = fmaf(__ldg(Lcol + a * n), x, dw[a]);
+        }
+        if (++f == n) {
+            const float t = (float)k * p.h;
+#pragma unroll 1
+            for (int a = 0; a < n; a++) {
+                if constexpr (MOD == MOD_MULTI) {
+                    const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * p.inv_S0), -p.alpha * t * kLog2e));
+                    S[a] = fmaf(S[a], fmaf(sl, dw[a], muh), S[a]);
+                } else {
+                    S[a] = fmaf(S[a], fmaf(__ldg(p.bsk + n + a), dw[a], muh), S[a]);
+                }
+                dw[a] = 0.f;
+            }
+            f = 0; k++;
+        }
+    }
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv) feed(p, z[i]);
+    }
+    __device__ __forceinline__ void step_dw(const KParams&, float, float) {}
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const int n = p.n_assets;
+        float b = 0.f;
+        if constexpr (MOD == MOD_MULTI) {
+#pragma unroll 1
+            for (int a = 0; a < n; a++) b += S[a];
+            b = b / (float)n;
+        } else {
+#pragma unroll 1
+            for (int a = 0; a < n; a++) b = fmaf(__ldg(p.bsk + 2 * n + a), S[a], b);
+        }
+        const float v = fmaxf(b - p.K, 0.f) * p.disc;
+        y[0] = v; y[1] = v * v;
+    }
+};
+
 // ------------------------------------------------------------------ Brownian bridge
 
 // Window of 32 increments from the bridge between W_L = W(32q) and W_R = W(32q + 32):

@@ -60,6 +60,13 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Greeks(C.Structure):
+    _fields_ = [("price", C.c_double), ("delta", C.c_double), ("rho", C.c_double), ("vega", C.c_double),
+                ("price_se", C.c_double), ("delta_se", C.c_double), ("rho_se", C.c_double),
+                ("vega_se", C.c_double), ("n_paths", C.c_int64), ("n_nodes", C.c_int32),
+                ("launches", C.c_int32), ("time_s", C.c_double), ("path_steps", C.c_double)]
+
+
 class CVPilotOut(C.Structure):
     _fields_ = [("beta", C.c_double), ("var_plain", C.c_double), ("var_cv", C.c_double)]
 
@@ -127,6 +134,17 @@ def basket_gbm(S0_vec, sigma_vec, L=None, weights=None, mu=0.05, T=1.0):
         m.weights = pw
         keep.append(w)
     return _keep(m, *keep)
+
+
+def config4_surface(seed=4, noise_sd=0.01):
+    """The local-vol surface of the adjoint workload: 64 strikes in [50, 150] x 32 times in [0, 2],
+    sigma(K, t) = 0.2 + 0.1 exp(-(K/100 - 1)^2 / 0.05) (1 + 0.5 t) plus seeded N(0, noise_sd^2)
+    noise (noise_sd read as the standard deviation), clipped below at 0.05."""
+    K = np.linspace(50.0, 150.0, 64)
+    t = np.linspace(0.0, 2.0, 32)
+    g = 0.2 + 0.1 * np.exp(-(K[None, :] / 100.0 - 1.0) ** 2 / 0.05) * (1.0 + 0.5 * t[:, None])
+    g = g + np.random.default_rng(seed).normal(0.0, noise_sd, g.shape)
+    return K, t, np.maximum(g, 0.05)
 
 
 def localvol_grid(K_axis, t_axis, sigma_grid, S0=100.0, mu=0.05, T=1.0):

@@ -142,6 +142,17 @@ typedef struct mcq_result {
 /* CVPilot (methods_cuda.cuh:94). */
 typedef struct mcq_cv_pilot_out { double beta, var_plain, var_cv; } mcq_cv_pilot_out;
 
+/* Pathwise adjoint Greeks (mcq_adjoint). */
+typedef struct mcq_greeks {
+    double price, delta, rho, vega;               /* means over all R x n_points paths */
+    double price_se, delta_se, rho_se, vega_se;   /* standard errors from the R replica means */
+    int64_t n_paths;
+    int32_t n_nodes;                              /* grid nodes written to node_vega (0 otherwise) */
+    int32_t launches;
+    double  time_s;
+    double  path_steps;                           /* forward + recompute + reverse path-steps */
+} mcq_greeks;
+
 typedef struct mcq_handle_s* mcq_handle;   /* opaque BB / PCA handle */
 
 /* ---------------------------------------------------------------- lifecycle */
@@ -198,6 +209,18 @@ int mcq_run_qmc_cv(const mcq_model* main_m, const mcq_model* ctrl_m, const mcq_p
 /* run_is_cuda (methods_cuda.cu:2285-2365): GBM European with drift shift z_star. */
 int mcq_run_is(const mcq_model* gbm, const mcq_payoff* european, double z_star, double eps,
                const mcq_mc_cfg* cfg, mcq_result* out);
+
+/* ---------------------------------------------------------------- sensitivities
+ * Pathwise adjoint Greeks over R scrambled-Sobol replicas (salts salt_base + r, points offset ..
+ * offset + n_points - 1); no counterpart in the reference, which computes no Greeks.
+ * delta = dV/dS0, rho = dV/d(rate) with the drift mu and the payoff's discount rate moving
+ * together, vega = dV/dsigma (GBM), dV/dsigma0 (parametric Dupire) or the parallel shift of the
+ * local-vol grid; node_vega (optional, lv_nt * lv_nK doubles, same layout as lv_sigma) receives
+ * dV/dsigma(K_i, t_j).  Lipschitz payoffs only: European, arithmetic Asian, lookback.
+ * n_steps: multiple of 32 in [32, 1024]; path states are checkpointed every 16 steps and
+ * recomputed in the reverse sweep. */
+int mcq_adjoint(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t salt_base, int R,
+                uint32_t offset, int64_t n_points, int flags, mcq_greeks* out, double* node_vega);
 
 /* ---------------------------------------------------------------- hot-path passes
  * One fused kernel pass over R replicas x n_points scrambled-Sobol points (salts
