@@ -13,6 +13,7 @@ from .mcq_types import (  # noqa: F401  (re-exported builders)
     GBM, HESTON, DUPIRE, MULTI_DUPIRE, LOCALVOL_GRID, BASKET_GBM,
     EUROPEAN, ASIAN, GEOM_ASIAN, LOOKBACK, BARRIER_UP_OUT, BASKET, BARRIER_DOWN_OUT,
     RAW, BB, PCA, FLAG_COMPAT_U_INF, FLAG_COMPAT_HESTON_MLMC,
+    BOOK_BATCHED, BOOK_PLAIN, book_option, config5_book,
     gbm, heston, dupire, multi_dupire, basket_gbm, localvol_grid, config4_surface, payoff, european, asian,
     geom_asian, lookback, barrier_up_out, barrier_down_out, basket, noise_dim,
 )
@@ -27,6 +28,7 @@ EXPORTS = [
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
     "mcq_mc_pass", "mcq_level_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
     "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_qmc_pass_noalloc", "mcq_adjoint",
+    "mcq_book_price", "mcq_book_level_sums",
 ]
 
 
@@ -250,6 +252,34 @@ def adjoint(m, p, n_steps, salt_base=42, R=16, offset=0, n_points=4096, flags=0)
     if nodes is not None:
         nodes = nodes.reshape(m.lv_nt, m.lv_nK)
     return d, nodes
+
+
+def book_price(options, mode=BOOK_BATCHED, ml=None, qc=None):
+    """mcq_book_price: MLQMC price and per-asset pathwise delta of every option of a book.
+    Returns (list of dicts {price, std_error, delta (n_assets,), n_samples, levels, converged},
+    stats dict).  ml / qc default to M = 2, pilot_n = 400, n0_steps = 1 and R = 16, salt 42."""
+    n = len(options)
+    arr = (T.BookOption * n)(*options)
+    out = (T.BookResult * n)()
+    st = T.BookStats()
+    ml = ml if ml is not None else mlmc_cfg(M=2, n0_steps=1)
+    qc = qc if qc is not None else qmc_cfg(R=16)
+    _check(lib().mcq_book_price(arr, C.c_int(n), C.byref(ml), C.byref(qc), C.c_int(mode), out, C.byref(st)))
+    res = []
+    for o, r in zip(options, out):
+        res.append({"price": r.price, "std_error": r.std_error, "delta": np.array(r.delta[:o.n_assets]),
+                    "n_samples": r.n_samples, "levels": r.levels, "converged": bool(r.converged)})
+    return res, st.as_dict()
+
+
+def book_level_sums(option, level, offset=0, n_points=1024, ml=None, qc=None):
+    """mcq_book_level_sums: [R][4 + n_assets] sums of one slice, through the book kernel."""
+    ml = ml if ml is not None else mlmc_cfg(M=2, n0_steps=1)
+    qc = qc if qc is not None else qmc_cfg(R=16)
+    out = np.zeros((qc.R, 20), np.float64)
+    _check(lib().mcq_book_level_sums(C.byref(option), C.byref(ml), C.byref(qc), C.c_int(level), C.c_uint32(offset),
+                                     C.c_int64(n_points), out.ctypes.data_as(_P(C.c_double))))
+    return out[:, :4 + option.n_assets]
 
 
 def mc_pass(m, p, n_steps, seed, stream_id, first_path, n_paths):

@@ -1,0 +1,647 @@
+// book.cu — a heterogeneous book of correlated GBM basket calls priced by MLQMC with the
+// pathwise delta per asset.  No counterpart in the reference, which rejects basket MLQMC
+// (methods_cuda.cu:1695-1697) and launches one option at a time with a stream per level
+// (:1745-1755).
+//
+// Each adaptive round collects, for every option still running, the (level, point range)
+// slices its MLQMC state machine needs next: the pilots, the optimal extra samples, the pilot
+// of a new level (the arithmetic of run_mlqmc_cuda, :1950-2000).  A slice covers all R
+// replicas (salts salt_base + l R + r, shared offsets) and is cut into chunks whose size
+// depends on the slice alone.  A persistent work-queue kernel per basket-width class (d <= 4,
+// <= 8, <= 16, each compiled for its own register budget) pulls chunks of every option and
+// level from an atomic counter; k_book_fin turns the chunk records of each slice into {mean of
+// the replica means of dY, their sample variance, per-asset mean delta}.  The round's kernels
+// are captured once in a CUDA graph and replayed with each round's slice list (the counts are
+// read on the device).
+//
+// The plain comparator runs the same kernels one option at a time, one launch per level on
+// that level's own stream — the reference's launch structure.  Chunk records depend only on
+// the slice, and each slice is reduced in a fixed order, so both modes give bit-identical
+// per-option results.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "book.h"
+#include "path_kernels.cuh"
+#include "support.h"
+
+namespace mcq {
+
+constexpr int kBookNST = 4 + kMaxBasket;   // BasketLevelC statistics per path
+constexpr int kBookOut = 2 + kMaxBasket;   // per slice: E dY, var of replica means, deltas
+constexpr int kBookMaxLevels = 12;
+constexpr int kBookMaxR = 32;
+constexpr int kBookClasses = 3;            // basket width <= 4, <= 8, <= 16
+constexpr int kChunkNormals = 8192;        // normals per lane a chunk aims at
+constexpr int kMaxChunksPerRep = 256;
+
+// hdr (int32): [0] n_specs, [1] n_chunks, [2 + c] first chunk of class c, [5] = n_chunks,
+// [6 + c] first slice of class c, [9] = n_specs, [10 + c] work-queue counter of class c.
+constexpr int kHdrInts = 16;
+
+struct BookOptDev {
+    double T;
+    float K, disc, mu;
+    int d, bsk_off, uncorrelated;
+};
+
+struct BookSpec {   // one (option, level) slice: all replicas, points [offset, offset + n_points)
+    int opt, level;
+    uint32_t offset, n_points;
+    int gpc, cpr, chunk0, pad;
+};
+
+struct BookArgs {
+    int* hdr;
+    const BookSpec* specs;
+    const BookOptDev* opts;
+    const float* bdata;
+    const uint32_t* dirs[kBookMaxLevels];
+    int dstride[kBookMaxLevels];
+    int R, M, n0;
+    float u_cap;
+    double* records;   // [chunk][kBookNST]
+    double* out;       // [slice][kBookOut]
+};
+
+__host__ __device__ inline int book_class(int d) { return d <= 4 ? 0 : (d <= 8 ? 1 : 2); }
+
+// Chunk c of the book: the KParams of its option and level, then the groups of its replica.
+template <int NB, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__ BookArgs a) {
+    constexpr int CLS = NB <= 4 ? 0 : (NB <= 8 ? 1 : 2);
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    constexpr int kpf = (int)((sizeof(KParams) + 15) / 16) * 4;   // KParams in floats
+    constexpr int per_warp = 1024 + kpf + 2 * kBookNST;
+    float* buf = reinterpret_cast<float*>(smem4) + wib * per_warp;
+    KParams* kp = reinterpret_cast<KParams*>(buf + 1024);
+    double* wrec = reinterpret_cast<double*>(buf + 1024 + kpf);
+    const int c_end = a.hdr[3 + CLS];
+    const int s_beg = a.hdr[6 + CLS], s_last = a.hdr[7 + CLS] - 1;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = a.hdr[2 + CLS] + atomicAdd(a.hdr + 10 + CLS, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= c_end) break;
+        int lo = s_beg, hi = s_last;   // last slice of the class with chunk0 <= c
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.specs[mid].chunk0 <= c) lo = mid; else hi = mid - 1;
+        }
+        const BookSpec s = a.specs[lo];
+        const int q = c - s.chunk0, r = q / s.cpr, j = q - r * s.cpr;
+        if (lane == 0) {
+            const BookOptDev o = a.opts[s.opt];
+            int nf = a.n0;
+            for (int l = 0; l < s.level; l++) nf *= a.M;
+            KParams& k = *kp;
+            memset(&k, 0, sizeof(KParams));
+            k.gen = GEN_SOBOL; k.noise = NOISE_RAW; k.model = MOD_BASKET; k.est = EST_COUPLED;
+            k.n_steps = nf; k.d_noise = o.d; k.D = nf * o.d; k.dstride = a.dstride[s.level];
+            k.n_coarse = s.level ? nf / a.M : 0;
+            k.M = s.level ? a.M : INT_MAX;   // the coarse path never steps on level 0
+            k.T = (float)o.T;
+            k.h = (float)(o.T / nf);
+            k.sqrt_h = sqrtf(k.h);
+            k.hc = (float)(o.T / max(k.n_coarse, 1));
+            k.mu = o.mu; k.K = o.K; k.disc = o.disc; k.pay_T = k.T;
+            k.n_assets = o.d; k.uncorrelated = o.uncorrelated; k.bsk = a.bdata + o.bsk_off;
+            k.u_cap = a.u_cap;
+            k.offset = s.offset; k.n_points = s.n_points;
+            k.dirs = a.dirs[s.level];
+        }
+        __syncwarp();
+        const KParams p = *kp;
+        const uint64_t g0 = s.offset >> 5;
+        const uint64_t gend = ((uint64_t)s.offset + s.n_points - 1) / 32 + 1;
+        const uint64_t gb = g0 + (uint64_t)j * (uint64_t)s.gpc;
+        const uint64_t ge = min(gb + (uint64_t)s.gpc, gend);
+        const uint32_t* dr = p.dirs + (size_t)r * 33 * (size_t)p.dstride;
+        AccWarp<kBookNST> wacc;
+        wacc.bind(wrec, lane);
+        for (uint64_t h = gb; h < ge; h++) {
+            const uint64_t n = h * 32 + (uint64_t)lane;
+            BasketLevelC<NB> cons;
+            cons.init(p);
+            run_group<GEN_SOBOL, NOISE_RAW>(p, cons, dr, 0u, h, n, buf, nullptr, lane);
+            float y[kBookNST];
+            cons.finish(p, y);
+            wacc.add(y, n >= p.offset && n < p.offset + p.n_points, lane);
+        }
+        wacc.flush(a.records + (size_t)c * kBookNST, lane);
+    }
+}
+
+// Per slice: replica sums from its chunk records in chunk order, then the mean of the replica
+// means of dY, their sample variance and the mean per-asset delta.  One warp per slice, one
+// lane per statistic.
+__global__ void k_book_fin(const __grid_constant__ BookArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int n_specs = a.hdr[0];
+    const int wpb = blockDim.x >> 5;
+    const int st = (lane == 0) ? 0 : (lane <= kMaxBasket ? 3 + lane : -1);   // dY or a delta
+    for (int s = blockIdx.x * wpb + (threadIdx.x >> 5); s < n_specs; s += gridDim.x * wpb) {
+        if (st < 0) continue;
+        const BookSpec sp = a.specs[s];
+        double rep[kBookMaxR];
+        double m = 0.0;
+        for (int r = 0; r < a.R; r++) {
+            double v = 0.0;
+            for (int j = 0; j < sp.cpr; j++) v += a.records[(size_t)(sp.chunk0 + r * sp.cpr + j) * kBookNST + st];
+            rep[r] = v / (double)sp.n_points;
+            m += rep[r];
+        }
+        m /= a.R;
+        double* o = a.out + (size_t)s * kBookOut;
+        if (lane == 0) {
+            double v = 0.0;
+            for (int r = 0; r < a.R; r++) v += (rep[r] - m) * (rep[r] - m);
+            o[0] = m;
+            o[1] = a.R > 1 ? v / (a.R - 1) : 0.0;
+        } else {
+            o[1 + lane] = m;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host
+
+void book_validate(const mcq_book_option* opts, int n, const mcq_mlmc_cfg& ml, const mcq_qmc_cfg& qc) {
+    MCQ_REQUIRE(opts && n >= 1, MCQ_ERR_INVALID, "book: needs at least one option");
+    MCQ_REQUIRE(qc.R >= 2 && qc.R <= kBookMaxR, MCQ_ERR_UNSUPPORTED, "book: R must be 2..32 replicas");
+    MCQ_REQUIRE(ml.M >= 2 && ml.n0_steps >= 1 && ml.pilot_n >= 1, MCQ_ERR_INVALID,
+                "book: needs M >= 2, n0_steps >= 1, pilot_n >= 1");
+    for (int i = 0; i < n; i++) {
+        const mcq_book_option& o = opts[i];
+        const std::string tag = "book option " + std::to_string(i) + ": ";
+        MCQ_REQUIRE(o.n_assets >= 1 && o.n_assets <= kMaxBasket, MCQ_ERR_UNSUPPORTED, tag + "needs 1..16 assets");
+        MCQ_REQUIRE(o.max_L >= 2 && o.max_L < kBookMaxLevels, MCQ_ERR_INVALID, tag + "max_L must be 2..11");
+        MCQ_REQUIRE(o.eps > 0 && o.T > 0 && o.S0 && o.sigma, MCQ_ERR_INVALID, tag + "needs eps > 0, T > 0, S0, sigma");
+        long long nf = ml.n0_steps;
+        for (int l = 0; l < o.max_L && nf <= 20000; l++) nf *= ml.M;
+        MCQ_REQUIRE(nf * o.n_assets <= 20000, MCQ_ERR_RANGE,
+                    tag + "finest level x assets exceeds the 20000 Sobol dimensions of the table");
+    }
+}
+
+namespace {
+
+constexpr int kIterCap = 50;   // run_mlqmc_cuda's iteration cap (:1950)
+
+size_t book_smem() {
+    const int kpf = (int)((sizeof(KParams) + 15) / 16) * 4;
+    return (size_t)kWarpsPerBlock * (1024 + kpf + 2 * kBookNST) * sizeof(float);
+}
+
+using BookFn = void (*)(BookArgs);
+BookFn book_fn(int cls) {
+    switch (cls) {
+        case 0: return k_book<4, 3>;
+        case 1: return k_book<8, 2>;
+        default: return k_book<16, 1>;
+    }
+}
+
+struct OptState {
+    int L = 2, iter = 0, phase = 0;   // phase 0: first pilots, 1: extras, 2: pilot of level L
+    bool done = false, converged = false;
+    double E[kBookMaxLevels] = {}, sig2[kBookMaxLevels] = {};
+    long long N[kBookMaxLevels] = {}, next_off[kBookMaxLevels] = {};
+    double Dl[kBookMaxLevels][kMaxBasket] = {};
+    int n_pending = 0;
+    int pend_level[kBookMaxLevels];
+    long long pend_n[kBookMaxLevels];
+};
+
+// Device and pinned buffers of one launch context (the batched round, or one level stream).
+struct Slot {
+    cudaStream_t stream = nullptr;
+    DevBuf specs, hdr, records, out;
+    PinnedBuf hspecs, hout;
+};
+
+}  // namespace
+
+struct BookRunner {
+    const mcq_book_option* opts = nullptr;
+    int n = 0;
+    mcq_mlmc_cfg ml{};
+    mcq_qmc_cfg qc{};
+    int R = 0, M = 0, n0 = 0, max_L_all = 2;
+    DevBuf d_opts, d_bdata;
+    std::vector<DevBuf> dirs;
+    std::vector<int> dstride;
+    std::vector<OptState> st;
+    size_t max_specs = 0;
+    long long launches = 0, rounds = 0;
+    double path_steps = 0;
+
+    long long nfine(int l) const {
+        long long v = n0;
+        for (int i = 0; i < l; i++) v *= M;
+        return v;
+    }
+
+    BookArgs args(Slot& s) const {
+        BookArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.hdr = (int*)s.hdr.p;
+        a.specs = (const BookSpec*)s.specs.p;
+        a.opts = (const BookOptDev*)d_opts.p;
+        a.bdata = (const float*)d_bdata.p;
+        for (int l = 0; l <= max_L_all; l++) {
+            a.dirs[l] = (const uint32_t*)dirs[l].p;
+            a.dstride[l] = dstride[l];
+        }
+        a.R = R; a.M = M; a.n0 = n0;
+        a.u_cap = ((qc.flags | ml.flags) & MCQ_FLAG_COMPAT_U_INF) ? 1.0f : 0x1.fffffep-1f;
+        a.records = (double*)s.records.p;
+        a.out = (double*)s.out.p;
+        return a;
+    }
+
+    void setup() {
+        Engine& E = engine();
+        book_validate(opts, n, ml, qc);
+        R = qc.R; M = ml.M; n0 = ml.n0_steps;
+        std::vector<BookOptDev> ho(n);
+        std::vector<float> bd;
+        int dmax = 1;
+        for (int i = 0; i < n; i++) {
+            const mcq_book_option& o = opts[i];
+            const int d = o.n_assets;
+            ho[i] = BookOptDev{o.T, (float)o.K, (float)std::exp(-o.r * o.T), (float)o.r, d, (int)bd.size(),
+                               o.L ? 0 : 1};
+            for (int a = 0; a < d; a++) bd.push_back((float)o.S0[a]);
+            for (int a = 0; a < d; a++) bd.push_back((float)o.sigma[a]);
+            for (int a = 0; a < d; a++) bd.push_back(o.weights ? (float)o.weights[a] : 1.0f / d);
+            for (int a = 0; a < d; a++)
+                for (int b = 0; b < d; b++) bd.push_back(o.L ? (float)o.L[a * d + b] : (a == b ? 1.f : 0.f));
+            max_L_all = std::max(max_L_all, o.max_L);
+            dmax = std::max(dmax, d);
+        }
+        cudaStream_t s0 = E.ws(0).stream;
+        MCQ_CUDA(cudaMemcpyAsync(d_opts.ensure(sizeof(BookOptDev) * n), ho.data(), sizeof(BookOptDev) * n,
+                                 cudaMemcpyHostToDevice, s0));
+        MCQ_CUDA(cudaMemcpyAsync(d_bdata.ensure(sizeof(float) * bd.size()), bd.data(), sizeof(float) * bd.size(),
+                                 cudaMemcpyHostToDevice, s0));
+        // one scrambled table per level shared by all options; an option of d assets uses its
+        // first nfine(l) d dimensions, exactly the table run_mlqmc builds for it
+        dirs.resize(max_L_all + 1);
+        dstride.assign(max_L_all + 1, 0);
+        for (int l = 0; l <= max_L_all; l++) {
+            dstride[l] = (int)(dmax * nfine(l));
+            uint32_t* t = (uint32_t*)dirs[l].ensure(sizeof(uint32_t) * (size_t)R * 33 * dstride[l]);
+            launch_prescramble(E.d_dv, qc.salt_base + (uint32_t)(l * R), R, dstride[l], t, s0);
+        }
+        MCQ_CUDA(cudaStreamSynchronize(s0));
+        max_specs = (size_t)n * (max_L_all + 1);
+        st.assign(n, OptState());
+    }
+
+    // The next slices option i needs (run_mlqmc_cuda :1950-2000); steps that need no sample
+    // are taken on the host at once.
+    void plan(int i) {
+        OptState& s = st[i];
+        const mcq_book_option& o = opts[i];
+        s.n_pending = 0;
+        while (!s.done && s.n_pending == 0) {
+            if (s.phase == 0) {
+                for (int l = 0; l <= 2; l++) add_pending(s, l, ml.pilot_n);
+            } else if (s.phase == 2) {
+                add_pending(s, s.L, ml.pilot_n);
+            } else {
+                if (s.iter >= kIterCap) { s.done = true; break; }
+                double sum_term = 0.0;
+                for (int l = 0; l <= s.L; l++) sum_term += std::sqrt(s.sig2[l] * std::pow((double)M, l));
+                for (int l = 0; l <= s.L; l++) {
+                    const double Cl = std::pow((double)M, l);
+                    long long Nopt = (long long)std::ceil(2.0 / ((double)R * o.eps * o.eps) * std::sqrt(s.sig2[l] / Cl) *
+                                                          sum_term);
+                    Nopt = std::max(Nopt, 100LL);
+                    if (Nopt > s.N[l]) add_pending(s, l, Nopt - s.N[l]);
+                }
+                if (s.n_pending == 0) end_iteration(i);
+            }
+        }
+    }
+    static void add_pending(OptState& s, int l, long long nn) {
+        s.pend_level[s.n_pending] = l;
+        s.pend_n[s.n_pending++] = nn;
+    }
+
+    // Bias test and level growth at the end of an iteration of extras (:1983-1999).
+    void end_iteration(int i) {
+        OptState& s = st[i];
+        const int L = s.L;
+        s.iter++;
+        double bias = std::abs(s.E[L]) / std::max(M - 1, 1);
+        if (L >= 1) bias = std::max(bias, std::abs(s.E[L - 1]) * M / (double)std::max(M * (M - 1), 1));
+        if (bias < opts[i].eps / std::sqrt(2.0)) {
+            s.done = s.converged = true;
+        } else if (L < opts[i].max_L) {
+            s.L++;
+            s.phase = 2;
+        } else if (s.iter >= kIterCap) {
+            s.done = true;
+        }
+    }
+
+    // Merge a slice's {E dY, var of replica means, deltas} into level l (:1927-1944, :1972-1979).
+    void absorb(int i, int l, long long nn, const double* r) {
+        OptState& s = st[i];
+        if (s.N[l] == 0) {
+            s.E[l] = r[0];
+            s.sig2[l] = r[1] * (double)nn;
+            for (int a = 0; a < kMaxBasket; a++) s.Dl[l][a] = r[2 + a];
+        } else {
+            const double wo = (double)s.N[l], wn = (double)nn;
+            s.E[l] = (s.E[l] * wo + r[0] * wn) / (wo + wn);
+            s.sig2[l] = (s.sig2[l] * wo + r[1] * wn * wn) / (wo + wn);
+            for (int a = 0; a < kMaxBasket; a++) s.Dl[l][a] = (s.Dl[l][a] * wo + r[2 + a] * wn) / (wo + wn);
+        }
+        s.N[l] += nn;
+        s.next_off[l] += nn;
+    }
+
+    void step_done(int i) {
+        OptState& s = st[i];
+        if (s.phase != 1) s.phase = 1;
+        else end_iteration(i);
+    }
+
+    BookSpec make_spec(int i, int l, long long nn) {
+        OptState& s = st[i];
+        MCQ_REQUIRE((unsigned long long)(s.next_off[l] + nn) <= 0xFFFFFFFFull, MCQ_ERR_RANGE,
+                    "book option " + std::to_string(i) + ": level " + std::to_string(l) +
+                        " offset exceeds the 32-bit Sobol limit");
+        BookSpec x{};
+        x.opt = i;
+        x.level = l;
+        x.offset = (uint32_t)s.next_off[l];
+        x.n_points = (uint32_t)nn;
+        // chunk size from the slice alone: about kChunkNormals normals per lane, at most
+        // kMaxChunksPerRep chunks per replica
+        const long long D = (long long)opts[i].n_assets * nfine(l);
+        const uint64_t G = ((uint64_t)x.offset + x.n_points - 1) / 32 + 1 - (x.offset >> 5);
+        uint64_t gpc = (uint64_t)std::max<long long>(1, kChunkNormals / D);
+        gpc = std::max<uint64_t>(gpc, (G + kMaxChunksPerRep - 1) / kMaxChunksPerRep);
+        x.gpc = (int)gpc;
+        x.cpr = (int)((G + gpc - 1) / gpc);
+        path_steps += (double)R * (double)nn * (double)(nfine(l) + (l ? nfine(l) / M : 0));
+        return x;
+    }
+
+    // Order slices by width class, assign chunk ranges, upload slices and header on s.stream.
+    int upload(Slot& s, std::vector<BookSpec>& sp) {
+        std::stable_sort(sp.begin(), sp.end(), [&](const BookSpec& a, const BookSpec& b) {
+            return book_class(opts[a.opt].n_assets) < book_class(opts[b.opt].n_assets);
+        });
+        int* h = (int*)s.hspecs.ensure(sizeof(int) * kHdrInts + sizeof(BookSpec) * std::max<size_t>(sp.size(), 1));
+        std::memset(h, 0, sizeof(int) * kHdrInts);
+        BookSpec* hs = reinterpret_cast<BookSpec*>(h + kHdrInts);
+        int chunk = 0;
+        size_t k = 0;
+        for (int c = 0; c < kBookClasses; c++) {
+            h[2 + c] = chunk;
+            h[6 + c] = (int)k;
+            for (; k < sp.size() && book_class(opts[sp[k].opt].n_assets) == c; k++) {
+                sp[k].chunk0 = chunk;
+                MCQ_REQUIRE((long long)chunk + (long long)R * sp[k].cpr < INT_MAX, MCQ_ERR_RANGE, "book: chunk count overflow");
+                chunk += R * sp[k].cpr;
+                hs[k] = sp[k];
+            }
+        }
+        h[0] = (int)sp.size();
+        h[1] = h[5] = chunk;
+        h[9] = (int)sp.size();
+        s.specs.ensure(sizeof(BookSpec) * std::max<size_t>(max_specs, 1));
+        s.hdr.ensure(sizeof(int) * kHdrInts);
+        s.out.ensure(sizeof(double) * kBookOut * std::max<size_t>(max_specs, 1));
+        MCQ_CUDA(cudaMemcpyAsync(s.hdr.p, h, sizeof(int) * kHdrInts, cudaMemcpyHostToDevice, s.stream));
+        if (!sp.empty())
+            MCQ_CUDA(cudaMemcpyAsync(s.specs.p, hs, sizeof(BookSpec) * sp.size(), cudaMemcpyHostToDevice, s.stream));
+        return chunk;
+    }
+
+    static int grid_of(int cls) {
+        static int per_sm[kBookClasses] = {-1, -1, -1};
+        if (per_sm[cls] < 0) {
+            const void* fn = (const void*)book_fn(cls);
+            MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)book_smem()));
+            int b = 0;
+            MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, book_smem()));
+            MCQ_REQUIRE(b > 0, MCQ_ERR_INTERNAL, "book kernel does not fit on an SM");
+            per_sm[cls] = b;
+        }
+        return per_sm[cls] * engine().sm_count;
+    }
+
+    void launch_book(int cls, const BookArgs& a, int grid, cudaStream_t st_) {
+        void* argv[] = {(void*)&a};
+        MCQ_CUDA(cudaLaunchKernel((const void*)book_fn(cls), dim3(grid), dim3(kThreads), argv, book_smem(), st_));
+    }
+    void launch_fin(const BookArgs& a, int grid, cudaStream_t st_) {
+        void* argv[] = {(void*)&a};
+        MCQ_CUDA(cudaLaunchKernel((const void*)k_book_fin, dim3(grid), dim3(256), argv, 0, st_));
+    }
+
+    // ---- batched: one graph per book, replayed once per round
+    void run_batched() {
+        Engine& E = engine();
+        Slot s;
+        s.stream = E.ws(0).stream;
+        cudaStream_t side[2] = {E.ws(1).stream, E.ws(2).stream};
+        cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+        MCQ_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        for (auto& e : join) MCQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        cudaGraphExec_t exec = nullptr;
+        const void* captured_records = nullptr;
+        const int grid[kBookClasses] = {grid_of(0), grid_of(1), grid_of(2)};
+        std::vector<BookSpec> sp;
+        auto cleanup = [&]() {
+            if (exec) cudaGraphExecDestroy(exec);
+            cudaEventDestroy(fork);
+            for (auto& e : join) cudaEventDestroy(e);
+        };
+        try {
+            for (;;) {
+                sp.clear();
+                for (int i = 0; i < n; i++) {
+                    plan(i);
+                    for (int k = 0; k < st[i].n_pending; k++) sp.push_back(make_spec(i, st[i].pend_level[k], st[i].pend_n[k]));
+                }
+                if (sp.empty()) break;
+                long long chunks = 0;
+                for (auto& x : sp) chunks += (long long)R * x.cpr;
+                s.records.ensure(sizeof(double) * kBookNST * (size_t)std::max<long long>(chunks, 1));
+                upload(s, sp);
+                if (!exec || captured_records != s.records.p) {   // (re)capture when a buffer moved
+                    if (exec) { MCQ_CUDA(cudaGraphExecDestroy(exec)); exec = nullptr; }
+                    const BookArgs a = args(s);
+                    cudaGraph_t g = nullptr;
+                    MCQ_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+                    MCQ_CUDA(cudaEventRecord(fork, s.stream));
+                    for (int c = 0; c < 2; c++) MCQ_CUDA(cudaStreamWaitEvent(side[c], fork, 0));
+                    launch_book(0, a, grid[0], s.stream);
+                    launch_book(1, a, grid[1], side[0]);
+                    launch_book(2, a, grid[2], side[1]);
+                    for (int c = 0; c < 2; c++) {
+                        MCQ_CUDA(cudaEventRecord(join[c], side[c]));
+                        MCQ_CUDA(cudaStreamWaitEvent(s.stream, join[c], 0));
+                    }
+                    launch_fin(a, E.sm_count * 4, s.stream);
+                    MCQ_CUDA(cudaStreamEndCapture(s.stream, &g));
+                    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+                    cudaGraphDestroy(g);
+                    MCQ_CUDA(ie);
+                    captured_records = s.records.p;
+                }
+                MCQ_CUDA(cudaGraphLaunch(exec, s.stream));
+                double* ho = (double*)s.hout.ensure(sizeof(double) * kBookOut * sp.size());
+                MCQ_CUDA(cudaMemcpyAsync(ho, s.out.p, sizeof(double) * kBookOut * sp.size(), cudaMemcpyDeviceToHost,
+                                         s.stream));
+                MCQ_CUDA(cudaStreamSynchronize(s.stream));
+                launches += kBookClasses + 1;
+                rounds++;
+                for (size_t k = 0; k < sp.size(); k++) absorb(sp[k].opt, sp[k].level, sp[k].n_points, ho + k * kBookOut);
+                for (int i = 0; i < n; i++)
+                    if (!st[i].done && st[i].n_pending > 0) step_done(i);
+            }
+        } catch (...) {
+            cudaStreamSynchronize(s.stream);
+            cleanup();
+            throw;
+        }
+        cleanup();
+    }
+
+    // ---- plain: per option, one launch of the option's class kernel per level on its stream
+    void run_plain() {
+        Engine& E = engine();
+        std::vector<Slot> slots(max_L_all + 1);
+        for (int l = 0; l <= max_L_all; l++) slots[l].stream = E.ws(1 + l).stream;
+        std::vector<BookSpec> one(1);
+        for (int i = 0; i < n; i++) {
+            const int cls = book_class(opts[i].n_assets);
+            for (;;) {
+                plan(i);
+                OptState& s = st[i];
+                if (s.done) break;
+                int issued_l[kBookMaxLevels];
+                long long issued_n[kBookMaxLevels];
+                const int np = s.n_pending;
+                for (int k = 0; k < np; k++) {
+                    const int l = s.pend_level[k];
+                    Slot& sl = slots[l];
+                    one[0] = make_spec(i, l, s.pend_n[k]);
+                    sl.records.ensure(sizeof(double) * kBookNST * (size_t)R * one[0].cpr);
+                    const int chunks = upload(sl, one);
+                    const BookArgs a = args(sl);
+                    launch_book(cls, a, std::max(1, std::min(grid_of(cls), (chunks + kWarpsPerBlock - 1) / kWarpsPerBlock)),
+                                sl.stream);
+                    launch_fin(a, 1, sl.stream);
+                    double* ho = (double*)sl.hout.ensure(sizeof(double) * kBookOut);
+                    MCQ_CUDA(cudaMemcpyAsync(ho, a.out, sizeof(double) * kBookOut, cudaMemcpyDeviceToHost, sl.stream));
+                    issued_l[k] = l;
+                    issued_n[k] = s.pend_n[k];
+                    launches += 2;
+                }
+                for (int k = 0; k < np; k++) {
+                    MCQ_CUDA(cudaStreamSynchronize(slots[issued_l[k]].stream));
+                    absorb(i, issued_l[k], issued_n[k], (const double*)slots[issued_l[k]].hout.p);
+                }
+                rounds++;
+                step_done(i);
+            }
+        }
+    }
+
+    void results(mcq_book_result* out) const {
+        for (int i = 0; i < n; i++) {
+            const OptState& s = st[i];
+            mcq_book_result& r = out[i];
+            std::memset(&r, 0, sizeof(r));
+            double vs = 0.0;
+            long long Nt = 0;
+            for (int l = 0; l <= s.L; l++) {   // :2010-2016
+                r.price += s.E[l];
+                if (s.N[l]) vs += s.sig2[l] / ((double)s.N[l] * (double)R);
+                Nt += s.N[l] * R;
+                for (int a = 0; a < opts[i].n_assets; a++) r.delta[a] += s.Dl[l][a];
+            }
+            r.std_error = std::sqrt(vs);
+            r.n_samples = Nt;
+            r.levels = s.L + 1;
+            r.converged = s.converged ? 1 : 0;
+        }
+    }
+};
+
+void book_level_sums(const mcq_book_option& opt, const mcq_mlmc_cfg& ml, const mcq_qmc_cfg& qc, int level,
+                     uint32_t offset, long long n_points, double* sums_host) {
+    MCQ_REQUIRE(level >= 0 && level <= opt.max_L, MCQ_ERR_INVALID, "book: level beyond the option's max_L");
+    MCQ_REQUIRE(n_points >= 1, MCQ_ERR_INVALID, "book: n_points >= 1");
+    BookRunner b;
+    b.opts = &opt;
+    b.n = 1;
+    b.ml = ml;
+    b.qc = qc;
+    b.setup();
+    b.st[0].next_off[level] = offset;
+    Slot s;
+    s.stream = engine().ws(0).stream;
+    std::vector<BookSpec> one(1, b.make_spec(0, level, n_points));
+    s.records.ensure(sizeof(double) * kBookNST * (size_t)b.R * one[0].cpr);
+    const int chunks = b.upload(s, one);
+    const int cls = book_class(opt.n_assets);
+    b.launch_book(cls, b.args(s), BookRunner::grid_of(cls), s.stream);
+    std::vector<double> rec((size_t)chunks * kBookNST);
+    MCQ_CUDA(cudaMemcpyAsync(rec.data(), s.records.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.stream));
+    MCQ_CUDA(cudaStreamSynchronize(s.stream));
+    engine().launches += 1;
+    for (int r = 0; r < b.R; r++)
+        for (int q = 0; q < kBookNST; q++) {
+            double v = 0.0;
+            for (int j = 0; j < one[0].cpr; j++) v += rec[(size_t)(r * one[0].cpr + j) * kBookNST + q];
+            sums_host[(size_t)r * kBookNST + q] = v;
+        }
+}
+
+void book_price(const mcq_book_option* opts, int n, const mcq_mlmc_cfg& ml, const mcq_qmc_cfg& qc, int mode,
+                mcq_book_result* out, mcq_book_stats* stats) {
+    MCQ_REQUIRE(out, MCQ_ERR_INVALID, "book: needs an output array");
+    MCQ_REQUIRE(mode == MCQ_BOOK_BATCHED || mode == MCQ_BOOK_PLAIN, MCQ_ERR_INVALID, "book: unknown mode");
+    const auto t0 = std::chrono::steady_clock::now();
+    BookRunner b;
+    b.opts = opts;
+    b.n = n;
+    b.ml = ml;
+    b.qc = qc;
+    b.setup();
+    const auto t1 = std::chrono::steady_clock::now();
+    if (mode == MCQ_BOOK_BATCHED) b.run_batched();
+    else b.run_plain();
+    MCQ_CUDA(cudaDeviceSynchronize());
+    MCQ_CUDA(cudaGetLastError());
+    const auto t2 = std::chrono::steady_clock::now();
+    b.results(out);
+    engine().launches += (int)b.launches;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->time_s = std::chrono::duration<double>(t2 - t1).count();
+        stats->setup_s = std::chrono::duration<double>(t1 - t0).count();
+        stats->path_steps = b.path_steps;
+        stats->rounds = (int)b.rounds;
+        stats->launches = (int)b.launches;
+    }
+}
+
+}  // namespace mcq

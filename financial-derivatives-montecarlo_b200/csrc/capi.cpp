@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "book.h"
 #include "drivers.h"
 #include "support.h"
 
@@ -424,7 +425,8 @@ int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, i
     a.offset = offset; a.n_points = (uint64_t)n_points; a.flags = flags;
     ensure_ready();
     auto s = pass_sync(engine().ws(0), a);
-    std::memcpy(sums_host, s.data(), sizeof(double) * s.size());
+    const int ns = nstat_of(EST_COUPLED, m->kind);   // basket records also carry per-asset deltas
+    for (int r = 0; r < R; r++) std::memcpy(sums_host + 4 * r, s.data() + (size_t)ns * r, 4 * sizeof(double));
     API_END
 }
 
@@ -461,6 +463,30 @@ int mcq_adjoint(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t s
     MCQ_REQUIRE(n_points >= 1 && R >= 1, MCQ_ERR_INVALID, "bad R / n_points");
     ensure_ready();
     adjoint_run(*m, *p, n_steps, salt_base, R, offset, (uint64_t)n_points, flags, *out, node_vega);
+    API_END
+}
+
+int mcq_book_price(const mcq_book_option* opts, int n, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc,
+                   int mode, mcq_book_result* out, mcq_book_stats* stats) {
+    API_BEGIN
+    NEED(opts); NEED(ml); NEED(qc); NEED(out);
+    MCQ_REQUIRE(mode == MCQ_BOOK_BATCHED || mode == MCQ_BOOK_PLAIN, MCQ_ERR_INVALID, "book: unknown mode");
+    book_validate(opts, n, *ml, *qc);
+    ensure_ready();
+    book_price(opts, n, *ml, *qc, mode, out, stats);
+    API_END
+}
+
+int mcq_book_level_sums(const mcq_book_option* opt, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc, int level,
+                        uint32_t offset, int64_t n_points, double* sums_host) {
+    API_BEGIN
+    NEED(opt); NEED(ml); NEED(qc); NEED(sums_host);
+    book_validate(opt, 1, *ml, *qc);
+    MCQ_REQUIRE(level >= 0 && level <= opt->max_L, MCQ_ERR_INVALID, "book: level beyond the option's max_L");
+    MCQ_REQUIRE(n_points >= 1 && (uint64_t)offset + (uint64_t)n_points <= (1ull << 32), MCQ_ERR_RANGE,
+                "book: n_points >= 1 and offset + n_points <= 2^32");
+    ensure_ready();
+    book_level_sums(*opt, *ml, *qc, level, offset, n_points, sums_host);
     API_END
 }
 

@@ -171,8 +171,9 @@ void run_qmc(const mcq_model& m, const mcq_payoff& p, double eps, int n_steps,
 void run_mlmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_mlmc_cfg& cfg,
               mcq_result& out) {
     check_model_payoff(m, p);
-    MCQ_REQUIRE(m.kind != MCQ_MODEL_MULTI_DUPIRE && m.kind != MCQ_MODEL_BASKET_GBM, MCQ_ERR_UNSUPPORTED,
-                "run_mlmc: baskets are not supported (as methods_cuda.cu:1318-1320)");
+    MCQ_REQUIRE(m.kind != MCQ_MODEL_MULTI_DUPIRE, MCQ_ERR_UNSUPPORTED,
+                "run_mlmc: the Dupire basket has no coupled path (as methods_cuda.cu:1318-1320); the "
+                "correlated GBM basket does");
     MCQ_REQUIRE(eps > 0 && cfg.M >= 2 && cfg.max_L >= 2 && cfg.pilot_n >= 1 && cfg.n0_steps >= 1,
                 MCQ_ERR_INVALID, "run_mlmc: bad eps / M / max_L / pilot_n / n0_steps");
     auto t0 = Clock::now();
@@ -199,7 +200,7 @@ void run_mlmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_mlm
         a.m = &m; a.p = &p; a.n_steps = (int)nf; a.est = EST_COUPLED; a.M = M; a.level0 = (l == 0);
         a.mlmc_h = true; a.gen = GEN_PHILOX; a.R = 1; a.offset = 0; a.n_points = (uint64_t)n;
         a.seed = cfg.seed; a.stream0 = seed_ctr++; a.flags = cfg.flags;
-        dsum[l] = (double*)w.sums.ensure(4 * sizeof(double));
+        dsum[l] = (double*)w.sums.ensure((size_t)nstat_of(EST_COUPLED, m.kind) * sizeof(double));
         pass_async(w, a, dsum[l]);
         ps += (double)n * (double)(nf + (l ? nf / M : 0));
     };
@@ -207,7 +208,7 @@ void run_mlmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_mlm
     auto collect = [&](int l) -> std::vector<double> {
         Workspace& w = engine().ws(1 + l);
         double* h = (double*)w.hsums.ensure(4 * sizeof(double));
-        MCQ_CUDA(cudaMemcpyAsync(h, dsum[l], 4 * sizeof(double), cudaMemcpyDeviceToHost, w.stream));
+        MCQ_CUDA(cudaMemcpyAsync(h, dsum[l], 4 * sizeof(double), cudaMemcpyDeviceToHost, w.stream));   // first 4 stats
         MCQ_CUDA(cudaStreamSynchronize(w.stream));
         return std::vector<double>(h, h + 4);
     };
@@ -283,8 +284,9 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
                const mcq_qmc_cfg& qc, int noise, const std::vector<const Handle*>& bb_list,
                const std::vector<const Handle*>& pca_list, mcq_result& out) {
     check_model_payoff(m, p);
-    MCQ_REQUIRE(m.kind != MCQ_MODEL_MULTI_DUPIRE && m.kind != MCQ_MODEL_BASKET_GBM, MCQ_ERR_UNSUPPORTED,
-                "run_mlqmc: baskets are not supported (as methods_cuda.cu:1695-1697)");
+    MCQ_REQUIRE(m.kind != MCQ_MODEL_MULTI_DUPIRE, MCQ_ERR_UNSUPPORTED,
+                "run_mlqmc: the Dupire basket has no coupled path (as methods_cuda.cu:1695-1697); the "
+                "correlated GBM basket does");
     MCQ_REQUIRE(noise == MCQ_NOISE_RAW || noise_dim(m) == 1, MCQ_ERR_UNSUPPORTED,
                 "run_mlqmc: Brownian bridge / PCA only for one-factor models (:1702-1704)");
     MCQ_REQUIRE(eps > 0 && ml.M >= 2 && ml.max_L >= 2 && ml.pilot_n >= 1 && ml.n0_steps >= 1 && qc.R >= 1,
@@ -292,6 +294,7 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
     auto t0 = Clock::now();
     const int l0c = engine().launches;
     const int M = ml.M, max_L = ml.max_L, R = qc.R;
+    const int ns = nstat_of(EST_COUPLED, m.kind);   // record stride per replica
     int L = 2;
     std::vector<double> E(max_L + 1, 0.0), sig2(max_L + 1, 0.0);
     std::vector<long long> N(max_L + 1, 0), next_off(max_L + 1, 0);
@@ -337,7 +340,7 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
         a.seed = qc.salt_base; a.stream0 = qc.salt_base + (uint32_t)(l * R);
         a.offset = (uint64_t)next_off[l];
         a.n_points = (uint64_t)n;
-        dsum[l] = (double*)w.sums.ensure((size_t)R * 4 * sizeof(double));
+        dsum[l] = (double*)w.sums.ensure((size_t)R * ns * sizeof(double));
         pass_async(w, a, dsum[l]);
         next_off[l] += n;
         ps += (double)R * (double)n * (double)(nf + (l ? nf / M : 0));
@@ -345,15 +348,15 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
     // collect_level (:1927-1944): mean and sample variance of the R replica means
     auto collect = [&](int l, long long n) -> std::pair<double, double> {
         Workspace& w = engine().ws(1 + l);
-        double* h = (double*)w.hsums.ensure((size_t)R * 4 * sizeof(double));
-        MCQ_CUDA(cudaMemcpyAsync(h, dsum[l], (size_t)R * 4 * sizeof(double), cudaMemcpyDeviceToHost, w.stream));
+        double* h = (double*)w.hsums.ensure((size_t)R * ns * sizeof(double));
+        MCQ_CUDA(cudaMemcpyAsync(h, dsum[l], (size_t)R * ns * sizeof(double), cudaMemcpyDeviceToHost, w.stream));
         MCQ_CUDA(cudaStreamSynchronize(w.stream));
         double mm = 0.0;
-        for (int r = 0; r < R; r++) mm += h[4 * r] / n;
+        for (int r = 0; r < R; r++) mm += h[ns * r] / n;
         mm /= R;
         double v = 0.0;
         for (int r = 0; r < R; r++) {
-            const double q = h[4 * r] / n - mm;
+            const double q = h[ns * r] / n - mm;
             v += q * q;
         }
         v = (R > 1) ? v / (R - 1) : 0.0;

@@ -132,6 +132,11 @@ int noise_dim(const mcq_model& m) {   // model_noise_dim, models.hpp:78-87
     }
 }
 
+int nstat_of(int est, int model) {
+    if (est == EST_COUPLED && model == MCQ_MODEL_BASKET_GBM) return 4 + kMaxBasket;
+    return nstat_of(est);
+}
+
 int nstat_of(int est) {
     switch (est) {
         case EST_COUPLED: return 4;
@@ -179,8 +184,9 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
     k.n_steps = a.n_steps;
     k.d_noise = noise_dim(m);
     k.D = a.n_steps * k.d_noise;
+    k.dstride = k.D;
     k.flags = a.flags;
-    k.nstat = nstat_of(a.est);
+    k.nstat = nstat_of(a.est, m.kind);
 
     const float Tf = (float)m.T;
     const float h = a.mlmc_h ? (float)(m.T / a.n_steps) : Tf / (float)a.n_steps;
@@ -307,7 +313,7 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     MCQ_REQUIRE(a.R >= 1, MCQ_ERR_INVALID, "R must be >= 1");
     MCQ_REQUIRE(a.m->T > 0, MCQ_ERR_INVALID, "T must be > 0");
     if (a.n_points == 0) {
-        MCQ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * a.R * nstat_of(a.est), ws.stream));
+        MCQ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * a.R * nstat_of(a.est, a.m->kind), ws.stream));
         return;
     }
     KParams k;
@@ -431,7 +437,8 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     }
 
     const int skel = (a.noise == NOISE_BB && D > 32) ? ((D >> 5) + 1) * 32 : 0;
-    const size_t smem = (size_t)kWarpsPerBlock * (1024 + skel) * sizeof(float);
+    const int accf = (!a.dump && a.est == EST_COUPLED && k.model == MOD_BASKET) ? ((2 * nst + 3) & ~3) : 0;
+    const size_t smem = (size_t)kWarpsPerBlock * (1024 + skel + accf) * sizeof(float);
     KernelInfo& ki = kernel_info(fn, smem);
     long long blocks = ((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock;
     blocks = std::min<long long>(blocks, (long long)ki.blocks_per_sm * E.sm_count);
@@ -508,7 +515,7 @@ static void check_err_word(Workspace& ws) {
 }
 
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a) {
-    const size_t n = (size_t)a.R * (a.dump ? 1 : nstat_of(a.est));
+    const size_t n = (size_t)a.R * (a.dump ? 1 : nstat_of(a.est, a.m->kind));
     double* d = (double*)ws.sums.ensure(sizeof(double) * n);
     pass_async(ws, a, d);
     double* h = (double*)ws.hsums.ensure(sizeof(double) * n);

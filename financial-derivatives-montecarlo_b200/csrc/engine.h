@@ -138,6 +138,7 @@ int noise_dim(const mcq_model& m);
 // KParams for a pass (make_params); basket / local-vol arrays are uploaded into ws.aux.
 void fill_params(Workspace& ws, const PassArgs& a, KParams& k);
 int nstat_of(int est);
+int nstat_of(int est, int model_kind);   // basket levels carry per-asset deltas
 // Enqueue one pass on ws.stream; d_out receives [R][nstat] doubles (device).
 void pass_async(Workspace& ws, const PassArgs& a, double* d_out);
 // Tensor-core PCA pass (N in {64, 128, 256}); called by pass_async.

@@ -68,9 +68,11 @@ struct KParams {
     const int2* bbi;
     // ---- PCA: M_pca (fp16, K-major rows = output step) device pointer
     const void* pca;
-    // ---- Sobol: pre-scrambled words, replica r at dirs + r * 33 * D, word k of dim d at
-    //      [k * D + d] (k = 32 is the digital shift)
+    // ---- Sobol: pre-scrambled words, replica r at dirs + r * 33 * dstride, word k of dim d at
+    //      [k * dstride + d] (k = 32 is the digital shift); dstride >= D (the table may cover more
+    //      dimensions than this pass uses, as the book's per-level tables do)
     const uint32_t* dirs;
+    int dstride;
     // ---- Philox
     uint32_t seed, stream_base;
     // ---- output: per-item partial sums [n_items][nstat]

@@ -185,6 +185,32 @@ struct Acc {
     }
 };
 
+// Accumulator for consumers with many statistics: each group's 32 values are reduced in FP32
+// by shuffles and lane 0 adds the group total to an FP64 record in the warp's shared memory.
+template <int NST>
+struct AccWarp {
+    double* rec;
+    __device__ __forceinline__ void bind(double* r, int lane) {
+        rec = r;
+        if (lane < NST) rec[lane] = 0.0;
+        __syncwarp();
+    }
+    __device__ __forceinline__ void add(const float (&y)[NST], bool valid, int lane) {
+#pragma unroll
+        for (int i = 0; i < NST; i++) {
+            float v = valid ? y[i] : 0.f;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) rec[i] += (double)v;
+        }
+    }
+    __device__ __forceinline__ void flush(double* out, int lane) {
+        __syncwarp();
+        if (lane < NST) out[lane] = rec[lane];
+        __syncwarp();
+    }
+};
+
 // ------------------------------------------------------------------ models and payoffs
 
 __device__ __forceinline__ float lv_sigma(const KParams& p, float S, float t) {
@@ -540,6 +566,96 @@ struct DumpC {
     __device__ __forceinline__ void finish(const KParams&, float (&y)[NST]) { y[0] = 0.f; }
 };
 
+// Coupled fine / coarse correlated GBM basket for MLMC / MLQMC levels (the reference refuses
+// baskets there, methods_cuda.cu:1318-1320, :1695-1697), with the pathwise delta per asset.
+// Euler GBM is linear in S0_a, so dS_a(T)/dS0_a = S_a(T)/S0_a and
+// delta_a = disc 1{B > K} w_a S_a(T) / S0_a on each of the fine and coarse paths.
+// Statistics: {dY, dY^2, Yf, Yf^2, d delta_0 .. d delta_15}.
+template <int NB>
+struct BasketLevelC {
+    static constexpr int NST = 4 + kMaxBasket;
+    static constexpr bool WARP_ACC = true;
+    float Sf[NB], Sc[NB], dw[NB], acc[NB];
+    float muh_f, muh_c;
+    int f, m;
+    __device__ __forceinline__ void bind(int, uint64_t) {}
+    __device__ __forceinline__ void flush() {}
+    __device__ __forceinline__ void init(const KParams& p) {
+        const int n = p.n_assets;
+#pragma unroll
+        for (int a = 0; a < NB; a++) {
+            Sf[a] = Sc[a] = (a < n) ? __ldg(p.bsk + a) : 0.f;
+            dw[a] = acc[a] = 0.f;
+        }
+        muh_f = p.mu * p.h;
+        muh_c = p.mu * p.hc;
+        f = 0; m = 0;
+    }
+    __device__ __forceinline__ void feed(const KParams& p, float z) {
+        const int n = p.n_assets;
+        const float x = z * p.sqrt_h;
+        if (p.uncorrelated) {
+#pragma unroll
+            for (int a = 0; a < NB; a++) if (a == f) dw[a] = x;
+        } else {
+            const float* Lcol = p.bsk + 3 * n + f;
+#pragma unroll
+            for (int a = 0; a < NB; a++)
+                if (a >= f && a < n) dw[a] = fmaf(__ldg(Lcol + a * n), x, dw[a]);
+        }
+        if (++f == n) {
+            const bool coarse = (++m == p.M);
+#pragma unroll
+            for (int a = 0; a < NB; a++) {
+                if (a < n) {
+                    const float sg = __ldg(p.bsk + n + a);
+                    Sf[a] = fmaf(Sf[a], fmaf(sg, dw[a], muh_f), Sf[a]);
+                    acc[a] += dw[a];
+                    if (coarse) {
+                        Sc[a] = fmaf(Sc[a], fmaf(sg, acc[a], muh_c), Sc[a]);
+                        acc[a] = 0.f;
+                    }
+                }
+                dw[a] = 0.f;
+            }
+            if (coarse) m = 0;
+            f = 0;
+        }
+    }
+    __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+            if (i < nv) feed(p, z[i]);
+    }
+    __device__ __forceinline__ void step_dw(const KParams&, float, float) {}
+    __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
+        const int n = p.n_assets;
+        float Bf = 0.f, Bc = 0.f;
+#pragma unroll
+        for (int a = 0; a < NB; a++)
+            if (a < n) {
+                const float w = __ldg(p.bsk + 2 * n + a);
+                Bf = fmaf(w, Sf[a], Bf);
+                Bc = fmaf(w, Sc[a], Bc);
+            }
+        const bool has_c = p.n_coarse > 0;
+        const float yf = fmaxf(Bf - p.K, 0.f) * p.disc;
+        const float yc = has_c ? fmaxf(Bc - p.K, 0.f) * p.disc : 0.f;
+        const float dy = yf - yc;
+        y[0] = dy; y[1] = dy * dy; y[2] = yf; y[3] = yf * yf;
+        const float gf = (Bf > p.K) ? p.disc : 0.f, gc = (has_c && Bc > p.K) ? p.disc : 0.f;
+#pragma unroll
+        for (int a = 0; a < kMaxBasket; a++) {
+            float v = 0.f;
+            if (a < NB && a < n) {
+                const float wa = __ldg(p.bsk + 2 * n + a) / __ldg(p.bsk + a);
+                v = wa * (gf * Sf[a] - gc * Sc[a]);
+            }
+            y[4 + a] = v;
+        }
+    }
+};
+
 // Wide basket (up to kMaxWideBasket assets, e.g. the reference's 100-asset example): the same
 // arithmetic as BasketC with the per-asset state in local memory and rolled loops.
 constexpr int kMaxWideBasket = 128;
@@ -646,7 +762,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         for (int d0 = 0; d0 < D; d0 += 32) {
             float z[32];
             if constexpr (GEN == GEN_SOBOL) {
-                sobol_tile(dr, D, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
                 __syncwarp();
                 read_row(buf, lane, z);
                 __syncwarp();
@@ -659,7 +775,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         // N <= 32 (one tile): dW_i = sum_k M[i][k] z_k with z and M rounded to fp16 as the
         // reference's cast + GEMM (methods_cuda.cu:1228-1229); larger N runs in k_pca.
         const int N = D;
-        sobol_tile(dr, D, lane, lane < N, h, p.u_cap, buf, lane);
+        sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane);
         __syncwarp();
         float z[32];
         read_row(buf, lane, z);
@@ -681,7 +797,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         const int N = D;
         if (N <= 32) {
             // one tile: the literal table-driven bridge (bb_apply, utils.cpp:104-124)
-            sobol_tile(dr, D, lane, lane < N, h, p.u_cap, buf, lane);
+            sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane);
             __syncwarp();
             float z[32];
             read_row(buf, lane, z);
@@ -707,7 +823,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
             const int S = N >> 5;
             skel[lane] = 0.f;
             for (int t0 = 0; t0 < S; t0 += 32) {
-                sobol_tile(dr, D, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane);
                 __syncwarp();
                 float z[32];
                 read_row(buf, lane, z);
@@ -731,7 +847,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
                     const int u = 31 - __clz(lane + 1);
                     dim = (S << u) + (q << u) + (lane + 1 - (1 << u));
                 }
-                sobol_tile(dr, D, dim, act, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, dim, act, h, p.u_cap, buf, lane);
                 __syncwarp();
                 float z[32];
                 read_row(buf, lane, z);
@@ -745,14 +861,22 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
 // MINB: resident CTAs per SM the register budget is set for (0: 2 for the bridge, whose
 // window keeps 33 W values live, kMinBlocks otherwise).  Variants differ only in register
 // allocation and scheduling, never in arithmetic, so they produce identical sums.
+template <class C>
+struct warp_acc_of { static constexpr bool value = false; };
+template <int NB>
+struct warp_acc_of<BasketLevelC<NB>> { static constexpr bool value = true; };
+
 template <int GEN, int NOISE, class C, int MINB = 0>
 __global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ? 2 : kMinBlocks))
     k_pass(const __grid_constant__ KParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    constexpr bool WACC = warp_acc_of<C>::value;
     const int skel_floats = (NOISE == NOISE_BB && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;
-    float* buf = reinterpret_cast<float*>(smem4) + wib * (1024 + skel_floats);
+    const int acc_floats = WACC ? ((2 * C::NST + 3) & ~3) : 0;
+    float* buf = reinterpret_cast<float*>(smem4) + wib * (1024 + skel_floats + acc_floats);
     float* skel = buf + 1024;
+    double* wrec = reinterpret_cast<double*>(buf + 1024 + skel_floats);
     const int total_warps = gridDim.x * kWarpsPerBlock;
     const uint64_t gend_all = p.g0 + p.G;
     for (int item = blockIdx.x * kWarpsPerBlock + wib; item < p.n_items; item += total_warps) {
@@ -760,10 +884,12 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ?
         const int j = item - r * p.items_per_rep;
         const uint64_t gb = p.g0 + (uint64_t)j * (uint64_t)p.gpi;
         const uint64_t ge = min(gb + (uint64_t)p.gpi, gend_all);
-        const uint32_t* dr = (GEN == GEN_SOBOL) ? p.dirs + (size_t)r * 33 * (size_t)p.D : nullptr;
+        const uint32_t* dr = (GEN == GEN_SOBOL) ? p.dirs + (size_t)r * 33 * (size_t)p.dstride : nullptr;
         const uint32_t stream = p.stream_base + (uint32_t)r;
-        Acc<C::NST> acc;
-        acc.zero();
+        Acc<WACC ? 1 : C::NST> acc;
+        AccWarp<C::NST> wacc;
+        if constexpr (WACC) wacc.bind(wrec, lane);
+        else acc.zero();
         for (uint64_t h = gb; h < ge; h++) {
             const uint64_t n = h * 32 + (uint64_t)lane;
             C cons;
@@ -773,9 +899,12 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ?
             run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane);
             float y[C::NST];
             cons.finish(p, y);
-            if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
+            const bool valid = n >= p.offset && n < p.offset + p.n_points;
+            if constexpr (WACC) wacc.add(y, valid, lane);
+            else if (valid) acc.add(y);
         }
-        acc.flush(p.partials + (size_t)item * C::NST, lane);
+        if constexpr (WACC) wacc.flush(p.partials + (size_t)item * C::NST, lane);
+        else acc.flush(p.partials + (size_t)item * C::NST, lane);
     }
 }
 

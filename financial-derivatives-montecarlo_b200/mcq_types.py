@@ -67,6 +67,29 @@ class Greeks(C.Structure):
                 ("launches", C.c_int32), ("time_s", C.c_double), ("path_steps", C.c_double)]
 
 
+BOOK_MAX_ASSETS = 16
+BOOK_BATCHED, BOOK_PLAIN = 0, 1
+
+
+class BookOption(C.Structure):
+    _fields_ = [("n_assets", C.c_int32), ("max_L", C.c_int32), ("K", C.c_double), ("r", C.c_double),
+                ("T", C.c_double), ("eps", C.c_double), ("S0", _pd), ("sigma", _pd), ("weights", _pd),
+                ("L", _pd)]
+
+
+class BookResult(C.Structure):
+    _fields_ = [("price", C.c_double), ("std_error", C.c_double), ("delta", C.c_double * BOOK_MAX_ASSETS),
+                ("n_samples", C.c_int64), ("levels", C.c_int32), ("converged", C.c_int32)]
+
+
+class BookStats(C.Structure):
+    _fields_ = [("time_s", C.c_double), ("setup_s", C.c_double), ("path_steps", C.c_double),
+                ("rounds", C.c_int32), ("launches", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class CVPilotOut(C.Structure):
     _fields_ = [("beta", C.c_double), ("var_plain", C.c_double), ("var_cv", C.c_double)]
 
@@ -145,6 +168,53 @@ def config4_surface(seed=4, noise_sd=0.01):
     g = 0.2 + 0.1 * np.exp(-(K[None, :] / 100.0 - 1.0) ** 2 / 0.05) * (1.0 + 0.5 * t[:, None])
     g = g + np.random.default_rng(seed).normal(0.0, noise_sd, g.shape)
     return K, t, np.maximum(g, 0.05)
+
+
+def book_option(S0, sigma, K, r, T, eps, max_L, weights=None, L=None):
+    """One basket call of a book: max(sum_a w_a S_a(T) - K, 0) e^{-rT} on correlated GBM assets
+    (L: lower Cholesky factor of the correlation, row-major; None: uncorrelated)."""
+    o = BookOption()
+    s0, p0 = _arr(S0)
+    sg, ps = _arr(sigma)
+    d = len(s0)
+    keep = [s0, sg]
+    o.n_assets, o.max_L, o.K, o.r, o.T, o.eps = d, int(max_L), K, r, T, eps
+    o.S0, o.sigma = p0, ps
+    if weights is not None:
+        w, pw = _arr(weights)
+        o.weights = pw
+        keep.append(w)
+    if L is not None:
+        l, pl = _arr(np.asarray(L, dtype=np.float64).reshape(d, d))
+        o.L = pl
+        keep.append(l)
+    return _keep(o, *keep)
+
+
+def config5_book(n=4096, seed=5, r=0.03):
+    """The batched heterogeneous book: n basket calls, d ~ U{1..16}, S0_i = 100 U[0.8, 1.2],
+    sigma_i ~ U[0.1, 0.5], correlation from a seeded A A^T + 0.5 I normalised to unit diagonal
+    (its Cholesky factor is passed), weights ~ Dirichlet(1), K = U[0.8, 1.2] x the weighted
+    forward, T ~ U[0.1, 3], 2^k steps with k ~ U{4..9} on the finest level (n0 = 1, M = 2, so
+    max_L = k), eps ~ U[5e-4, 5e-3].  r is common to the book (the workload leaves it open)."""
+    rng = np.random.default_rng(seed)
+    book = []
+    for _ in range(n):
+        d = int(rng.integers(1, 17))
+        S0 = 100.0 * rng.uniform(0.8, 1.2, d)
+        sig = rng.uniform(0.1, 0.5, d)
+        A = rng.normal(size=(d, d))
+        Cm = A @ A.T + 0.5 * np.eye(d)
+        dg = np.sqrt(np.diag(Cm))
+        corr = Cm / np.outer(dg, dg)
+        L = np.linalg.cholesky(corr)
+        w = rng.dirichlet(np.ones(d))
+        T = float(rng.uniform(0.1, 3.0))
+        K = float(rng.uniform(0.8, 1.2) * np.dot(w, S0) * np.exp(r * T))
+        k = int(rng.integers(4, 10))
+        eps = float(rng.uniform(5e-4, 5e-3))
+        book.append(book_option(S0, sig, K, r, T, eps, k, weights=w, L=L))
+    return book
 
 
 def localvol_grid(K_axis, t_axis, sigma_grid, S0=100.0, mu=0.05, T=1.0):

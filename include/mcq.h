@@ -16,8 +16,8 @@
  *   - `stream` arguments are cudaStream_t passed as void*; NULL means the engine's own
  *     internal stream.
  *   - The engine uses the CUDA device selected by mcq_init() (default: current device).
- *   - Not re-entrant per handle: two threads must not share one BB/PCA handle or one
- *     book object at the same time.  Distinct handles may be used concurrently.
+ *   - Not re-entrant per handle: two threads must not share one BB/PCA handle at the same
+ *     time.  Distinct handles may be used concurrently.
  */
 #ifndef MCQ_H
 #define MCQ_H
@@ -37,7 +37,6 @@ extern "C" {
 #define MCQ_ERR_NOMEM        5   /* device or host allocation failed                 */
 #define MCQ_ERR_INTERNAL     6
 #define MCQ_ERR_TIMEOUT      7   /* a bounded device-side wait gave up               */
-#define MCQ_ERR_CANCELLED    8   /* a book run was cancelled                         */
 
 /* ---------------------------------------------------------------- enumerations */
 /* Model kinds.  0..3 follow ModelKind (methods_cuda.cu:205); 4, 5 are engine additions. */
@@ -153,6 +152,39 @@ typedef struct mcq_greeks {
     double  path_steps;                           /* forward + recompute + reverse path-steps */
 } mcq_greeks;
 
+/* One option of a batched book (mcq_book_price): a call on a weighted basket of correlated
+   GBM assets, max(sum_a w_a S_a(T) - K, 0) e^{-rT}, drift r, priced by MLQMC to its own eps
+   with the pathwise delta per asset.  No counterpart in the reference. */
+#define MCQ_BOOK_MAX_ASSETS 16
+typedef struct mcq_book_option {
+    int32_t n_assets;             /* 1..16 */
+    int32_t max_L;                /* finest level, 2..11; level l has n0_steps * M^l steps */
+    double K, r, T, eps;
+    const double* S0;             /* [n_assets] */
+    const double* sigma;          /* [n_assets] */
+    const double* weights;        /* [n_assets]; NULL: equal weights */
+    const double* L;              /* [n_assets^2] row-major lower Cholesky; NULL: uncorrelated */
+} mcq_book_option;
+
+typedef struct mcq_book_result {
+    double  price, std_error;     /* sum over levels of the level means; SE as run_mlqmc */
+    double  delta[MCQ_BOOK_MAX_ASSETS];   /* pathwise d price / d S0_a, first n_assets used */
+    int64_t n_samples;            /* sum over levels of N_l x R */
+    int32_t levels;               /* L + 1 */
+    int32_t converged;            /* 1: the bias test passed before the iteration cap */
+} mcq_book_result;
+
+typedef struct mcq_book_stats {
+    double  time_s;               /* pricing time, after the per-book set-up */
+    double  setup_s;              /* parameter upload and scrambled tables */
+    double  path_steps;           /* sum over slices of R x points x (fine + coarse steps) */
+    int32_t rounds;               /* adaptive rounds (batched) / per-option steps (plain) */
+    int32_t launches;             /* kernel launches issued */
+} mcq_book_stats;
+
+#define MCQ_BOOK_BATCHED  0       /* every option and level in one graph replay per round */
+#define MCQ_BOOK_PLAIN    1       /* one option at a time, one launch per level on its stream */
+
 typedef struct mcq_handle_s* mcq_handle;   /* opaque BB / PCA handle */
 
 /* ---------------------------------------------------------------- lifecycle */
@@ -222,6 +254,17 @@ int mcq_run_is(const mcq_model* gbm, const mcq_payoff* european, double z_star, 
 int mcq_adjoint(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t salt_base, int R,
                 uint32_t offset, int64_t n_points, int flags, mcq_greeks* out, double* node_vega);
 
+/* Batched book: prices n options by MLQMC (the adaptive level / sample logic of
+ * run_mlqmc_cuda, methods_cuda.cu:1950-2000, per option; R = qc->R replicas with salts
+ * qc->salt_base + l R + r; M, pilot_n, n0_steps from ml; ml->max_L is ignored in favour of
+ * each option's own).  MCQ_BOOK_BATCHED runs every option's pending slices of a round in one
+ * persistent work-queue kernel replayed from a CUDA graph; MCQ_BOOK_PLAIN is the per-option,
+ * stream-per-level form (methods_cuda.cu:1745-1755) with the same kernels.  Both give
+ * bit-identical results.  No counterpart in the reference (which rejects basket MLQMC,
+ * methods_cuda.cu:1695-1697).  stats may be NULL. */
+int mcq_book_price(const mcq_book_option* opts, int n, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc,
+                   int mode, mcq_book_result* out, mcq_book_stats* stats);
+
 /* ---------------------------------------------------------------- hot-path passes
  * One fused kernel pass over R replicas x n_points scrambled-Sobol points (salts
  * salt_base + r, point indices offset .. offset + n_points - 1).  sums_host receives
@@ -282,6 +325,12 @@ int mcq_pca_matrix(mcq_handle pca, float* M_colmajor_f32);
 int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_handle bb,
                         int use_sobol, uint32_t seed, uint32_t salt_base, int R, uint32_t offset,
                         int64_t n_points, int flags, float* out_host);
+/* The book kernel's per-replica sums over one slice of one option (level `level`, points
+   offset .. offset + n_points - 1, R = qc->R replicas with salts qc->salt_base + level R + r):
+   sums_host[R][20] = {sum dY, sum dY^2, sum Yf, sum Yf^2, sum d(dY)/dS0_a for a < 16 (0 beyond
+   n_assets)}.  For parity tests of the book against the oracle. */
+int mcq_book_level_sums(const mcq_book_option* opt, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc, int level,
+                        uint32_t offset, int64_t n_points, double* sums_host);
 
 #ifdef __cplusplus
 }

@@ -725,6 +725,101 @@ int orc_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M,
     return 0;
 }
 
+/* Coupled fine/coarse pair of a correlated GBM basket call (per-asset sigma; the correlated
+ * increments L z sqrt(h) of correlate_multi_dupire, methods_cuda.cu:1097-1148; fine and coarse
+ * paths driven by the same increments as kernel_mlmc, :445-518) in FP64, with the pathwise
+ * sensitivities to each S0_a.  Euler is linear in S0_a, so dS_a(T)/dS0_a = S_a(T)/S0_a and
+ * d payoff/dS0_a = disc 1{B > K} w_a S_a(T)/S0_a.  z: normals in order step * n + asset.
+ * M <= 0: level 0 (no coarse path).  Returns Yf; *yc = Yc; dd[a] = d(Yf - Yc)/dS0_a. */
+double orc_basket_level(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, const double* z,
+                        double* yc, double* dd) {
+    int n = m->n_assets, coarse = M > 0, Mr = coarse ? M : 1;
+    int n_coarse = coarse ? n_fine / Mr : 0;
+    double hf = m->T / n_fine, hc = m->T / (n_coarse > 0 ? n_coarse : 1), sq = sqrt(hf);
+    double *Sf = (double*)malloc(sizeof(double) * 4 * n), *Sc = Sf + n, *dw = Sf + 2 * n, *acc = Sf + 3 * n;
+    for (int a = 0; a < n; a++) { Sf[a] = Sc[a] = m->S0_vec[a]; acc[a] = 0; }
+    int unc = m->uncorrelated || !m->L;
+    for (int k = 0; k < n_fine; k++) {
+        for (int a = 0; a < n; a++) {
+            double v = 0;
+            if (unc) v = z[k * n + a] * sq;
+            else for (int j = 0; j <= a; j++) v += m->L[a * n + j] * z[k * n + j] * sq;
+            dw[a] = v;
+        }
+        for (int a = 0; a < n; a++) {
+            Sf[a] = Sf[a] + m->mu * Sf[a] * hf + m->sigma_vec[a] * Sf[a] * dw[a];
+            acc[a] += dw[a];
+        }
+        if (coarse && (k + 1) % Mr == 0) {
+            for (int a = 0; a < n; a++) {
+                Sc[a] = Sc[a] + m->mu * Sc[a] * hc + m->sigma_vec[a] * Sc[a] * acc[a];
+                acc[a] = 0;
+            }
+        }
+    }
+    double Bf = 0, Bc = 0, disc = pay_discount(p);
+    for (int a = 0; a < n; a++) {
+        double w = m->weights ? m->weights[a] : 1.0 / n;
+        Bf += w * Sf[a];
+        Bc += w * Sc[a];
+    }
+    double yf = fmax(Bf - p->K, 0.0) * disc;
+    *yc = n_coarse > 0 ? fmax(Bc - p->K, 0.0) * disc : 0.0;
+    double gf = Bf > p->K ? disc : 0.0, gc = (n_coarse > 0 && Bc > p->K) ? disc : 0.0;
+    for (int a = 0; a < n; a++) {
+        double w = m->weights ? m->weights[a] : 1.0 / n;
+        dd[a] = w / m->S0_vec[a] * (gf * Sf[a] - gc * Sc[a]);
+    }
+    free(Sf);
+    return yf;
+}
+
+int orc_basket_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, uint32_t salt_base,
+                          int R, uint32_t offset, int64_t N, int flags, int n_threads, double* sums) {
+    int n = m->n_assets, D = n_fine * n, ns = 4 + n;
+    if (D > 20000) return -1;
+    if ((uint64_t)offset + (uint64_t)N > 0x100000000ull) return -2;
+    int nch = (N < ORC_CHUNKS) ? (int)(N > 0 ? N : 1) : ORC_CHUNKS;
+    double* part = (double*)calloc((size_t)R * nch * ns, sizeof(double));
+    uint32_t* Lv = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)R * D * 33);
+    for (int r = 0; r < R; r++)
+        for (int dd = 0; dd < D; dd++) {
+            uint32_t* w = Lv + ((size_t)r * D + dd) * 33;
+            prescramble(salt_base + (uint32_t)r, dd, w, w + 32);
+        }
+    int nt = n_threads > 0 ? n_threads : orc_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int64_t task = 0; task < (int64_t)R * nch; task++) {
+        int r = (int)(task / nch), c = (int)(task % nch);
+        int64_t b = N * c / nch, e = N * (c + 1) / nch;
+        if (b >= e) continue;
+        uint32_t* x = (uint32_t*)malloc(sizeof(uint32_t) * D);
+        double* z = (double*)malloc(sizeof(double) * (D + n));
+        double* dd = z + D;
+        const uint32_t* L = Lv + (size_t)r * D * 33;
+        for (int q = 0; q < D; q++) x[q] = scr_direct(L + q * 33, L[q * 33 + 32], offset + (uint32_t)b);
+        double* s = part + (size_t)task * ns;
+        for (int64_t i = b; i < e; i++) {
+            uint32_t idx = offset + (uint32_t)i;
+            if (i > b) { int k = __builtin_ctz(idx); for (int q = 0; q < D; q++) x[q] ^= L[q * 33 + k]; }
+            for (int q = 0; q < D; q++) z[q] = orc_ppnd16((double)orc_u_of(x[q], flags));
+            double yc, yf = orc_basket_level(m, p, n_fine, M, z, &yc, dd);
+            double dy = yf - yc;
+            s[0] += dy; s[1] += dy * dy; s[2] += yf; s[3] += yf * yf;
+            for (int a = 0; a < n; a++) s[4 + a] += dd[a];
+        }
+        free(x); free(z);
+    }
+    for (int r = 0; r < R; r++)
+        for (int q = 0; q < ns; q++) {
+            double a = 0;
+            for (int c = 0; c < nch; c++) a += part[((size_t)r * nch + c) * ns + q];
+            sums[r * ns + q] = a;
+        }
+    free(part); free(Lv);
+    return 0;
+}
+
 int orc_mc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t seed,
                 uint32_t stream, int64_t first_path, int64_t n_paths, int n_threads,
                 double* sums) {

@@ -79,6 +79,10 @@ double orc_path_payoff(const mcq_model* m, const mcq_payoff* p, int n_steps,
 double orc_level_payoff(const mcq_model* m, const mcq_payoff* p, int n_fine, int M,
                         const orc_noise* nz, const double* z, int flags, double* yc);
 
+/* coupled correlated GBM basket call with pathwise d(dY)/dS0_a in dd[n_assets]; M <= 0: level 0 */
+double orc_basket_level(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, const double* z,
+                        double* yc, double* dd);
+
 /* ---- drivers (sums over replicas/points; OpenMP) ---- */
 /* sums[R][2]: {sum Y, sum Y^2} over points offset..offset+N-1 of salts salt_base + r */
 int orc_qmc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, const orc_noise* nz,
@@ -88,6 +92,10 @@ int orc_qmc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, const orc
 int orc_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M,
                    const orc_noise* nz, int use_sobol, uint32_t seed, uint32_t salt_base,
                    int R, uint32_t offset, int64_t N, int flags, int n_threads, double* sums);
+/* sums[R][4 + n]: {sum dY, sum dY^2, sum Yf, sum Yf^2, sum d(dY)/dS0_a ...} over scrambled
+   Sobol points offset..offset+N-1 of salts salt_base + r (basket model, raw ordering) */
+int orc_basket_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, uint32_t salt_base,
+                          int R, uint32_t offset, int64_t N, int flags, int n_threads, double* sums);
 /* sums[2] over Philox paths first_path .. first_path + n_paths - 1 of (seed, stream) */
 int orc_mc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t seed,
                 uint32_t stream, int64_t first_path, int64_t n_paths, int n_threads,

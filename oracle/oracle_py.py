@@ -186,6 +186,27 @@ def level_sums(m, p, n_fine, M, nz=None, use_sobol=True, seed=42, salt_base=42, 
     return out
 
 
+def basket_level(m, p, n_fine, M, z):
+    """One coupled basket path pair: (Yf, Yc, dd[n_assets]); M <= 0 is level 0."""
+    z = np.ascontiguousarray(z, dtype=np.float64)
+    dd = np.zeros(m.n_assets)
+    yc = C.c_double()
+    L = lib()
+    L.orc_basket_level.restype = C.c_double
+    yf = L.orc_basket_level(C.byref(m), C.byref(p), C.c_int(n_fine), C.c_int(M), z.ctypes.data_as(_pd),
+                            C.byref(yc), dd.ctypes.data_as(_pd))
+    return yf, yc.value, dd
+
+
+def basket_level_sums(m, p, n_fine, M, salt_base=42, R=1, offset=0, N=1024, flags=0, threads=0):
+    out = np.zeros((R, 4 + m.n_assets))
+    rc = lib().orc_basket_level_sums(C.byref(m), C.byref(p), C.c_int(n_fine), C.c_int(M), C.c_uint32(salt_base),
+                                     C.c_int(R), C.c_uint32(offset), C.c_int64(N), C.c_int(flags), C.c_int(threads),
+                                     out.ctypes.data_as(_pd))
+    assert rc == 0, rc
+    return out
+
+
 def mc_sums(m, p, n_steps, seed, stream, first_path, n_paths, threads=0):
     out = np.zeros(2)
     lib().orc_mc_sums(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_uint32(seed), C.c_uint32(stream),

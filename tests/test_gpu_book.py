@@ -1,0 +1,137 @@
+"""Batched heterogeneous book through the C ABI: the book kernel's slice sums against the FP64
+oracle, batched == plain bit for bit, agreement with the single-option MLQMC driver, and
+prices / deltas against Black–Scholes for one-asset baskets."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _ncdf(x):
+    return 0.5 * math.erfc(-x / math.sqrt(2.0))
+
+
+def _basket(eng, d, seed, eps=2e-3, max_L=5, T=1.0, r=0.03, corr=True, kmul=1.0):
+    rng = np.random.default_rng(seed)
+    S0 = 100 * rng.uniform(0.8, 1.2, d)
+    sig = rng.uniform(0.1, 0.5, d)
+    A = rng.normal(size=(d, d))
+    Cm = A @ A.T + 0.5 * np.eye(d)
+    dg = np.sqrt(np.diag(Cm))
+    Lc = np.linalg.cholesky(Cm / np.outer(dg, dg)) if corr else None
+    w = rng.dirichlet(np.ones(d))
+    K = float(kmul * (w @ S0) * np.exp(r * T))
+    o = eng.book_option(S0, sig, K, r, T, eps, max_L, weights=w, L=Lc)
+    return o, (S0, sig, Lc, w, K, r, T)
+
+
+@pytest.mark.parametrize("d,level,corr", [(1, 0, True), (3, 1, True), (4, 3, False), (7, 2, True),
+                                          (12, 1, True), (16, 4, True)])
+def test_book_slice_sums_match_oracle(gpu, orc, d, level, corr):
+    """Per-replica sums of one slice (ragged offset and count) through the book kernel against
+    the FP64 oracle of the coupled basket pair with pathwise deltas."""
+    o, (S0, sig, Lc, w, K, r, T) = _basket(gpu, d, 100 + d, corr=corr)
+    ml, qc = gpu.mlmc_cfg(M=2, n0_steps=1), gpu.qmc_cfg(R=4, salt_base=42)
+    offset, N = 37, 1000
+    g = gpu.book_level_sums(o, level, offset, N, ml, qc)
+    m = gpu.basket_gbm(S0, sig, L=Lc, weights=w, mu=r, T=T)
+    p = gpu.basket(K, r, T, d)
+    ref = orc.basket_level_sums(m, p, 2 ** level, 2 if level else 0, salt_base=42 + level * 4, R=4,
+                                offset=offset, N=N)
+    # FP32 paths against FP64: 2e-5 of the per-point scale of the payoff (columns 0, 2) and
+    # of its square (columns 1, 3), summed over the N points
+    for q in range(4):
+        scale = N + abs(ref[:, 3 if q in (1, 3) else 2]).max()
+        assert np.abs(g[:, q] - ref[:, q]).max() < 2e-5 * scale, (q, g[:, q], ref[:, q])
+    # deltas: a path whose basket sits within FP32 rounding of K may flip its indicator
+    assert np.abs(g[:, 4:] - ref[:, 4:]).max() < 3.0 + 1e-4 * N, (g[:, 4:], ref[:, 4:])
+
+
+def test_book_batched_equals_plain_bit_for_bit(gpu):
+    book = gpu.config5_book(n=24, seed=77)
+    for o in book:
+        o.eps = 10 * o.eps                       # keep the test short: coarser targets
+    rb, sb = gpu.book_price(book, gpu.BOOK_BATCHED)
+    rp, sp = gpu.book_price(book, gpu.BOOK_PLAIN)
+    for a, b in zip(rb, rp):
+        assert a["price"] == b["price"] and a["std_error"] == b["std_error"]
+        assert a["n_samples"] == b["n_samples"] and a["levels"] == b["levels"]
+        assert np.array_equal(a["delta"], b["delta"])
+    assert sb["path_steps"] == sp["path_steps"]
+    assert sb["launches"] < sp["launches"]
+
+
+def test_book_matches_single_option_mlqmc(gpu):
+    """Each option of a book against run_mlqmc on the same basket (same points, same MLQMC
+    logic; only the order of the FP64 sums differs)."""
+    opts, models = [], []
+    for i, d in enumerate([1, 2, 5, 9, 16]):
+        o, (S0, sig, Lc, w, K, r, T) = _basket(gpu, d, 300 + i, eps=3e-3, max_L=6, T=0.5 + 0.4 * i)
+        opts.append(o)
+        models.append((gpu.basket_gbm(S0, sig, L=Lc, weights=w, mu=r, T=T), gpu.basket(K, r, T, d)))
+    res, _ = gpu.book_price(opts, gpu.BOOK_BATCHED, gpu.mlmc_cfg(M=2, n0_steps=1), gpu.qmc_cfg(R=16))
+    for o, (m, p), b in zip(opts, models, res):
+        ml = gpu.mlmc_cfg(M=2, n0_steps=1, max_L=o.max_L)
+        ref = gpu.run_mlqmc(m, p, o.eps, ml, gpu.qmc_cfg(R=16))
+        assert b["levels"] == ref["levels"] and b["n_samples"] == ref["n_samples"], (b, ref)
+        assert abs(b["price"] - ref["price"]) < 1e-7 * (1 + abs(ref["price"])), (b, ref)
+        assert abs(b["std_error"] - ref["std_error"]) < 1e-5 * ref["std_error"] + 1e-12
+
+
+@pytest.mark.parametrize("kmul,T", [(1.0, 1.0), (0.9, 2.0), (1.1, 0.5)])
+def test_book_one_asset_vs_black_scholes(gpu, orc, kmul, T):
+    """A one-asset basket is a European call: MLQMC price within 3 SE + 10 eps of Black–Scholes
+    (the stopping rule |E_L| / (M - 1) < eps / sqrt 2 of run_mlqmc_cuda bounds the Euler bias
+    only heuristically), pathwise delta within 1e-2 of N(d1)."""
+    o, (S0, sig, _, w, K, r, T) = _basket(gpu, 1, 7, eps=1e-3, max_L=8, T=T, kmul=kmul)
+    (res,), _ = gpu.book_price([o], gpu.BOOK_BATCHED)
+    S, s = float(S0[0]), float(sig[0])
+    bs = orc.bs_call(S, K, T, r, s)
+    d1 = (math.log(S / K) + (r + 0.5 * s * s) * T) / (s * math.sqrt(T))
+    assert abs(res["price"] - bs) < 3 * res["std_error"] + 10 * o.eps, (res, bs)
+    assert abs(res["delta"][0] - _ncdf(d1)) < 1e-2, (res["delta"], _ncdf(d1))
+
+
+def test_book_delta_matches_bump_and_revalue(gpu):
+    """Pathwise deltas of a 6-asset slice against central differences of the same slice with
+    common scrambled points (bump 0.5% of S0)."""
+    o, (S0, sig, Lc, w, K, r, T) = _basket(gpu, 6, 900)
+    ml, qc = gpu.mlmc_cfg(M=2, n0_steps=4), gpu.qmc_cfg(R=8)
+    N = 1 << 14
+    g = gpu.book_level_sums(o, 0, 0, N, ml, qc)
+    for a in range(6):
+        h = 5e-3 * S0[a]
+        up, dn = S0.copy(), S0.copy()
+        up[a] += h
+        dn[a] -= h
+        ou = gpu.book_option(up, sig, K, r, T, o.eps, o.max_L, weights=w, L=Lc)
+        od = gpu.book_option(dn, sig, K, r, T, o.eps, o.max_L, weights=w, L=Lc)
+        fu = gpu.book_level_sums(ou, 0, 0, N, ml, qc)[:, 2].sum()
+        fd = gpu.book_level_sums(od, 0, 0, N, ml, qc)[:, 2].sum()
+        fdiff = (fu - fd) / (2 * h)
+        pw = g[:, 4 + a].sum()
+        assert abs(fdiff - pw) < 1e-2 * abs(pw) + 1e-3 * N * w[a], (a, fdiff, pw)
+
+
+def test_book_config5_sample_prices_converge(gpu):
+    """A sample of the synthetic book: every option converges, its SE meets its own eps, and
+    the one-asset options agree with Black–Scholes."""
+    book = gpu.config5_book(n=64, seed=5)
+    for o in book:
+        o.eps = 4 * o.eps                        # keep the test short: coarser targets
+    res, st = gpu.book_price(book, gpu.BOOK_BATCHED)
+    assert st["rounds"] >= 2 and st["launches"] == 4 * st["rounds"]
+    for o, r in zip(book, res):
+        assert np.isfinite(r["price"]) and r["price"] >= 0
+        assert r["std_error"] <= o.eps * 1.01 or not r["converged"], (o.eps, r)
+        if o.n_assets == 1:
+            S, s = o.S0[0], o.sigma[0]
+            assert abs(r["price"] - orc_bs(S, o.K, o.T, o.r, s)) < 3 * r["std_error"] + 10 * o.eps
+    assert sum(r["converged"] for r in res) >= 0.9 * len(res)
+
+
+def orc_bs(S, K, T, r, s):
+    d1 = (math.log(S / K) + (r + 0.5 * s * s) * T) / (s * math.sqrt(T))
+    return S * _ncdf(d1) - K * math.exp(-r * T) * _ncdf(d1 - s * math.sqrt(T))
