@@ -131,6 +131,31 @@ def cpu_baseline(seconds=12.0, steps=1):
             "sample": f"{REPS} replicas x {n} points x {STEPS} steps of the same workload (FP64 oracle)"}
 
 
+def book_bench(eng, n):
+    """The batched heterogeneous book against its plain form on the same GPU: the first n options
+    of the 4096-option synthetic book (d ~ U{1..16}, correlated GBM, Dirichlet weights, T ~
+    U[0.1, 3], 16-512 finest steps, eps ~ U[5e-4, 5e-3]), each priced by MLQMC (R = 16, M = 2)
+    with its per-asset pathwise deltas.  Each mode is timed by the library around its pricing
+    loop (host wall time with the device synchronised), after a warm-up book."""
+    book = eng.config5_book(n=4096, seed=5)[:n]
+    eng.book_price(book[:8], eng.BOOK_BATCHED)
+    eng.book_price(book[:8], eng.BOOK_PLAIN)
+    out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5); "
+                                     "MLQMC R=16 M=2 n0=1, per-option eps, price + per-asset delta" % n}
+    res = {}
+    for name, mode in (("batched", eng.BOOK_BATCHED), ("plain", eng.BOOK_PLAIN)):
+        r, st = eng.book_price(book, mode)
+        res[name] = r
+        out[name] = {"options_per_s": n / st["time_s"], "time_s": st["time_s"], "rounds": st["rounds"],
+                     "launches": st["launches"], "normals_per_s": st["normals"] / st["time_s"],
+                     "path_steps_per_s": st["path_steps"] / st["time_s"]}
+    out["batched_over_plain"] = out["batched"]["options_per_s"] / out["plain"]["options_per_s"]
+    out["bit_identical"] = all(a["price"] == b["price"] and bool((a["delta"] == b["delta"]).all())
+                               for a, b in zip(res["batched"], res["plain"]))
+    out["converged"] = sum(1 for x in res["batched"] if x["converged"])
+    return out
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
@@ -165,6 +190,8 @@ def main():
     ap.add_argument("--e2e-runs", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true", help="skip the bridge / PCA orderings")
+    ap.add_argument("--book-options", type=int, default=64,
+                    help="options of the synthetic basket book priced batched and plain (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -266,6 +293,8 @@ def main():
     e2e_value = world * e2e_ps / e2e_t
     doublings = max(1, int(round(__import__("math").log2(e2e_last["n_samples"] / (REPS << 14)))) + 1)
 
+    book = None if args.book_options <= 0 else book_bench(eng, args.book_options)
+
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -311,6 +340,8 @@ def main():
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
     }
+    if book is not None:
+        line["book"] = book
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)

@@ -7,8 +7,9 @@
 // slices its MLQMC state machine needs next: the pilots, the optimal extra samples, the pilot
 // of a new level (the arithmetic of run_mlqmc_cuda, :1950-2000).  A slice covers all R
 // replicas (salts salt_base + l R + r, shared offsets) and is cut into chunks whose size
-// depends on the slice alone.  A persistent work-queue kernel per basket-width class (d <= 4,
-// <= 8, <= 16, each compiled for its own register budget) pulls chunks of every option and
+// depends on the slice alone.  A persistent work-queue kernel per basket-width class (d in 1-4,
+// 5-8, 9-12, 13-16, each compiled for its own register budget and specialised on the exact d)
+// pulls chunks of every option and
 // level from an atomic counter; k_book_fin turns the chunk records of each slice into {mean of
 // the replica means of dY, their sample variance, per-asset mean delta}.  The round's kernels
 // are captured once in a CUDA graph and replayed with each round's slice list (the counts are
@@ -33,16 +34,16 @@
 
 namespace mcq {
 
-constexpr int kBookNST = 4 + kMaxBasket;   // BasketLevelC statistics per path
+constexpr int kBookNST = 4 + kMaxBasket;   // per-path statistics in a chunk record
 constexpr int kBookOut = 2 + kMaxBasket;   // per slice: E dY, var of replica means, deltas
 constexpr int kBookMaxLevels = 12;
 constexpr int kBookMaxR = 32;
-constexpr int kBookClasses = 3;            // basket width <= 4, <= 8, <= 16
+constexpr int kBookClasses = 4;            // basket width 1-4, 5-8, 9-12, 13-16
 constexpr int kChunkNormals = 8192;        // normals per lane a chunk aims at
 constexpr int kMaxChunksPerRep = 256;
 
-// hdr (int32): [0] n_specs, [1] n_chunks, [2 + c] first chunk of class c, [5] = n_chunks,
-// [6 + c] first slice of class c, [9] = n_specs, [10 + c] work-queue counter of class c.
+// hdr (int32): [0] n_specs, [1] n_chunks, [2 + c] first chunk of class c, [6] = n_chunks,
+// [7 + c] first slice of class c, [11] = n_specs, [12 + c] work-queue counter of class c.
 constexpr int kHdrInts = 16;
 
 struct BookOptDev {
@@ -61,33 +62,206 @@ struct BookArgs {
     int* hdr;
     const BookSpec* specs;
     const BookOptDev* opts;
-    const float* bdata;
+    const float* bdata;   // per option [S0 | sigma | weight | L (d x d row-major)]
     const uint32_t* dirs[kBookMaxLevels];
     int dstride[kBookMaxLevels];
     int R, M, n0;
     float u_cap;
-    double* records;   // [chunk][kBookNST]
-    double* out;       // [slice][kBookOut]
+    double* records;      // [chunk][kBookNST]
+    double* out;          // [slice][kBookOut]
 };
 
-__host__ __device__ inline int book_class(int d) { return d <= 4 ? 0 : (d <= 8 ? 1 : 2); }
+__host__ __device__ inline int book_class(int d) { return (d - 1) >> 2; }
 
-// Chunk c of the book: the KParams of its option and level, then the groups of its replica.
-template <int NB, int MINB>
+// Per-warp shared memory: the 32 x 32 transpose tile, the option's Cholesky factor with rows
+// padded to a multiple of 4 floats, and the FP64 record of the chunk.
+constexpr int kBookLsFloats = kMaxBasket * kMaxBasket;
+constexpr int kBookWarpFloats = 1024 + kBookLsFloats + 2 * kBookNST;
+
+// The coupled basket pair of one path for a basket of exactly D assets: the correlated Euler
+// step S + S (mu h + sigma dW) with dW = L x, x = z sqrt(h), coarse steps on the summed fine
+// increments every M fine steps, the call on the weighted basket and d payoff / d S0_a =
+// disc 1{B > K} w_a S_a(T) / S0_a.  Same operations in the same order as the fused pass's
+// coupled basket consumer, so a slice gives the values the single-option MLQMC driver gives.
+template <int D>
+struct BookPath {
+    static constexpr int DP = (D + 3) & ~3, NS = 4 + D;
+    float Sf[D], Sc[D], acc[D];
+    int m;
+    __device__ __forceinline__ void init(const float* bk) {
+#pragma unroll
+        for (int q = 0; q < D; q++) {
+            Sf[q] = Sc[q] = __ldg(bk + q);
+            acc[q] = 0.f;
+        }
+        m = 0;
+    }
+    // x: this step's D normals times sqrt(h); L4: lower Cholesky rows padded to DP floats
+    __device__ __forceinline__ void step(const float (&x)[D], const float4* L4, const float (&sg)[D], float muh_f,
+                                         float muh_c, int Mc) {
+#pragma unroll
+        for (int q = 0; q < D; q++) {
+            float dw = 0.f;
+#pragma unroll
+            for (int j4 = 0; j4 <= q / 4; j4++) {
+                const float4 v = L4[(q * DP) / 4 + j4];
+                dw = fmaf(v.x, x[4 * j4], dw);
+                if (4 * j4 + 1 <= q) dw = fmaf(v.y, x[4 * j4 + 1], dw);
+                if (4 * j4 + 2 <= q) dw = fmaf(v.z, x[4 * j4 + 2], dw);
+                if (4 * j4 + 3 <= q) dw = fmaf(v.w, x[4 * j4 + 3], dw);
+            }
+            Sf[q] = fmaf(Sf[q], fmaf(sg[q], dw, muh_f), Sf[q]);
+            acc[q] += dw;
+        }
+        if (++m == Mc) {
+#pragma unroll
+            for (int q = 0; q < D; q++) {
+                Sc[q] = fmaf(Sc[q], fmaf(sg[q], acc[q], muh_c), Sc[q]);
+                acc[q] = 0.f;
+            }
+            m = 0;
+        }
+    }
+    __device__ __forceinline__ void finish(const float* bk, float K, float disc, bool has_c, float (&y)[NS]) const {
+        float Bf = 0.f, Bc = 0.f;
+#pragma unroll
+        for (int q = 0; q < D; q++) {
+            const float w = __ldg(bk + 2 * D + q);
+            Bf = fmaf(w, Sf[q], Bf);
+            Bc = fmaf(w, Sc[q], Bc);
+        }
+        const float yf = fmaxf(Bf - K, 0.f) * disc;
+        const float yc = has_c ? fmaxf(Bc - K, 0.f) * disc : 0.f;
+        const float dy = yf - yc;
+        const float gf = (Bf > K) ? disc : 0.f, gc = (has_c && Bc > K) ? disc : 0.f;
+        y[0] = dy; y[1] = dy * dy; y[2] = yf; y[3] = yf * yf;
+#pragma unroll
+        for (int q = 0; q < D; q++) {
+            const float wa = __ldg(bk + 2 * D + q) / __ldg(bk + q);
+            y[4 + q] = wa * (gf * Sf[q] - gc * Sc[q]);
+        }
+    }
+};
+
+// Warp sum of one path's statistics into the chunk's FP64 record (lane 0 adds).
+template <int NS>
+__device__ __forceinline__ void book_acc(const float (&y)[NS], bool valid, double* wrec, int lane) {
+#pragma unroll
+    for (int q = 0; q < NS; q++) {
+        float v = valid ? y[q] : 0.f;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) wrec[q] += (double)v;
+    }
+}
+
+// One chunk of a slice for a basket of exactly D assets: groups [gb, ge) of replica r.
+//
+// Paths of Dt = nf D <= 16 normals (the low levels of baskets of up to 8 assets) take
+// Q = 32 / Dt groups per Sobol tile: lane j generates dimension j mod Dt of group g + j / Dt,
+// and each lane then steps its Q paths from the transposed tile.  Longer paths are generated
+// step-major: a tile holds S = 32 / D whole steps (W = S D dimensions, lane j < W owning
+// dimension k0 D + j), so every normal of a step sits in known registers after the transpose
+// and L x is an unrolled triangular product with L read as float4 broadcasts.
+template <int D>
+__device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s, const BookOptDev& o, int r,
+                                           uint64_t gb, uint64_t ge, float* buf, float* Ls, double* wrec,
+                                           double* rec, int lane) {
+    using P = BookPath<D>;
+    constexpr int S = 32 / D, W = S * D, DP = P::DP, NS = P::NS;
+    const float* bk = a.bdata + o.bsk_off;
+    for (int i = lane; i < D * DP; i += 32) {
+        const int row = i / DP, col = i - row * DP;
+        Ls[i] = (col <= row) ? __ldg(bk + 3 * D + row * D + col) : 0.f;
+    }
+    if (lane < NS) wrec[lane] = 0.0;
+    float sg[D];
+#pragma unroll
+    for (int q = 0; q < D; q++) sg[q] = __ldg(bk + D + q);
+    int nf = a.n0;
+    for (int l = 0; l < s.level; l++) nf *= a.M;
+    const int nc = s.level ? nf / a.M : 0;
+    const int Mc = s.level ? a.M : INT_MAX;   // the coarse path never steps on level 0
+    const float h = (float)(o.T / nf);
+    const float sqrt_h = sqrtf(h);
+    const float hc = (float)(o.T / max(nc, 1));
+    const float muh_f = o.mu * h, muh_c = o.mu * hc;
+    const float K = o.K, disc = o.disc;
+    const bool has_c = nc > 0;
+    const int dstride = a.dstride[s.level];
+    const uint32_t* dr = a.dirs[s.level] + (size_t)r * 33 * (size_t)dstride;
+    const int Dt = nf * D;
+    const uint64_t pend = (uint64_t)s.offset + s.n_points;
+    const float4* L4 = reinterpret_cast<const float4*>(Ls);
+    __syncwarp();
+    if (D <= 8 && 2 * Dt <= 32) {   // wider baskets keep their registers for the step-major path
+        const int Q = 32 / Dt, qj = lane / Dt, dj = lane - qj * Dt;
+        for (uint64_t g = gb; g < ge; g += Q) {
+            const uint64_t gl = g + (uint64_t)qj;
+            sobol_tile(dr, dstride, dj, qj < Q && gl < ge, gl, a.u_cap, buf, lane);
+            __syncwarp();
+            for (int q = 0; q < Q && g + q < ge; q++) {
+                P path;
+                path.init(bk);
+                for (int k = 0; k < nf; k++) {
+                    float x[D];
+#pragma unroll
+                    for (int c = 0; c < D; c++) x[c] = buf[swz(lane, q * Dt + k * D + c)] * sqrt_h;
+                    path.step(x, L4, sg, muh_f, muh_c, Mc);
+                }
+                float y[NS];
+                path.finish(bk, K, disc, has_c, y);
+                const uint64_t n = (g + q) * 32 + (uint64_t)lane;
+                book_acc<NS>(y, n >= s.offset && n < pend, wrec, lane);
+            }
+            __syncwarp();
+        }
+    } else {
+        for (uint64_t g = gb; g < ge; g++) {
+            P path;
+            path.init(bk);
+            for (int k0 = 0; k0 < nf; k0 += S) {
+                const int dim = k0 * D + lane;
+                sobol_tile(dr, dstride, dim, lane < W && dim < Dt, g, a.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+#pragma unroll
+                for (int st = 0; st < S; st++) {
+                    if (k0 + st < nf) {
+                        float x[D];
+#pragma unroll
+                        for (int c = 0; c < D; c++) x[c] = z[st * D + c] * sqrt_h;
+                        path.step(x, L4, sg, muh_f, muh_c, Mc);
+                    }
+                }
+            }
+            float y[NS];
+            path.finish(bk, K, disc, has_c, y);
+            const uint64_t n = g * 32 + (uint64_t)lane;
+            book_acc<NS>(y, n >= s.offset && n < pend, wrec, lane);
+        }
+    }
+    __syncwarp();
+    if (lane < kBookNST) rec[lane] = (lane < NS) ? wrec[lane] : 0.0;
+    __syncwarp();
+}
+
+// Persistent work-queue kernel of one width class: warps take chunks from the class's atomic
+// counter until the round's chunks run out.
+template <int CLS, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__ BookArgs a) {
-    constexpr int CLS = NB <= 4 ? 0 : (NB <= 8 ? 1 : 2);
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    constexpr int kpf = (int)((sizeof(KParams) + 15) / 16) * 4;   // KParams in floats
-    constexpr int per_warp = 1024 + kpf + 2 * kBookNST;
-    float* buf = reinterpret_cast<float*>(smem4) + wib * per_warp;
-    KParams* kp = reinterpret_cast<KParams*>(buf + 1024);
-    double* wrec = reinterpret_cast<double*>(buf + 1024 + kpf);
+    float* buf = reinterpret_cast<float*>(smem4) + wib * kBookWarpFloats;
+    float* Ls = buf + 1024;
+    double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats);
     const int c_end = a.hdr[3 + CLS];
-    const int s_beg = a.hdr[6 + CLS], s_last = a.hdr[7 + CLS] - 1;
+    const int s_beg = a.hdr[7 + CLS], s_last = a.hdr[8 + CLS] - 1;
     for (;;) {
         int c = 0;
-        if (lane == 0) c = a.hdr[2 + CLS] + atomicAdd(a.hdr + 10 + CLS, 1);
+        if (lane == 0) c = a.hdr[2 + CLS] + atomicAdd(a.hdr + 12 + CLS, 1);
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= c_end) break;
         int lo = s_beg, hi = s_last;   // last slice of the class with chunk0 <= c
@@ -96,46 +270,18 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
             if (a.specs[mid].chunk0 <= c) lo = mid; else hi = mid - 1;
         }
         const BookSpec s = a.specs[lo];
+        const BookOptDev o = a.opts[s.opt];
         const int q = c - s.chunk0, r = q / s.cpr, j = q - r * s.cpr;
-        if (lane == 0) {
-            const BookOptDev o = a.opts[s.opt];
-            int nf = a.n0;
-            for (int l = 0; l < s.level; l++) nf *= a.M;
-            KParams& k = *kp;
-            memset(&k, 0, sizeof(KParams));
-            k.gen = GEN_SOBOL; k.noise = NOISE_RAW; k.model = MOD_BASKET; k.est = EST_COUPLED;
-            k.n_steps = nf; k.d_noise = o.d; k.D = nf * o.d; k.dstride = a.dstride[s.level];
-            k.n_coarse = s.level ? nf / a.M : 0;
-            k.M = s.level ? a.M : INT_MAX;   // the coarse path never steps on level 0
-            k.T = (float)o.T;
-            k.h = (float)(o.T / nf);
-            k.sqrt_h = sqrtf(k.h);
-            k.hc = (float)(o.T / max(k.n_coarse, 1));
-            k.mu = o.mu; k.K = o.K; k.disc = o.disc; k.pay_T = k.T;
-            k.n_assets = o.d; k.uncorrelated = o.uncorrelated; k.bsk = a.bdata + o.bsk_off;
-            k.u_cap = a.u_cap;
-            k.offset = s.offset; k.n_points = s.n_points;
-            k.dirs = a.dirs[s.level];
-        }
-        __syncwarp();
-        const KParams p = *kp;
-        const uint64_t g0 = s.offset >> 5;
         const uint64_t gend = ((uint64_t)s.offset + s.n_points - 1) / 32 + 1;
-        const uint64_t gb = g0 + (uint64_t)j * (uint64_t)s.gpc;
+        const uint64_t gb = (s.offset >> 5) + (uint64_t)j * (uint64_t)s.gpc;
         const uint64_t ge = min(gb + (uint64_t)s.gpc, gend);
-        const uint32_t* dr = p.dirs + (size_t)r * 33 * (size_t)p.dstride;
-        AccWarp<kBookNST> wacc;
-        wacc.bind(wrec, lane);
-        for (uint64_t h = gb; h < ge; h++) {
-            const uint64_t n = h * 32 + (uint64_t)lane;
-            BasketLevelC<NB> cons;
-            cons.init(p);
-            run_group<GEN_SOBOL, NOISE_RAW>(p, cons, dr, 0u, h, n, buf, nullptr, lane);
-            float y[kBookNST];
-            cons.finish(p, y);
-            wacc.add(y, n >= p.offset && n < p.offset + p.n_points, lane);
+        double* rec = a.records + (size_t)c * kBookNST;
+        switch (o.d - 4 * CLS) {
+            case 1: book_chunk<4 * CLS + 1>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
+            case 2: book_chunk<4 * CLS + 2>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
+            case 3: book_chunk<4 * CLS + 3>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
+            default: book_chunk<4 * CLS + 4>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
         }
-        wacc.flush(a.records + (size_t)c * kBookNST, lane);
     }
 }
 
@@ -195,17 +341,16 @@ namespace {
 
 constexpr int kIterCap = 50;   // run_mlqmc_cuda's iteration cap (:1950)
 
-size_t book_smem() {
-    const int kpf = (int)((sizeof(KParams) + 15) / 16) * 4;
-    return (size_t)kWarpsPerBlock * (1024 + kpf + 2 * kBookNST) * sizeof(float);
-}
+size_t book_smem() { return (size_t)kWarpsPerBlock * kBookWarpFloats * sizeof(float); }
 
+// Resident CTAs per SM each width class is compiled for (its register budget).
 using BookFn = void (*)(BookArgs);
 BookFn book_fn(int cls) {
     switch (cls) {
-        case 0: return k_book<4, 3>;
-        case 1: return k_book<8, 2>;
-        default: return k_book<16, 1>;
+        case 0: return k_book<0, 3>;
+        case 1: return k_book<1, 2>;
+        case 2: return k_book<2, 2>;
+        default: return k_book<3, 2>;
     }
 }
 
@@ -241,7 +386,7 @@ struct BookRunner {
     std::vector<OptState> st;
     size_t max_specs = 0;
     long long launches = 0, rounds = 0;
-    double path_steps = 0;
+    double path_steps = 0, normals = 0;
 
     long long nfine(int l) const {
         long long v = n0;
@@ -396,6 +541,7 @@ struct BookRunner {
         x.gpc = (int)gpc;
         x.cpr = (int)((G + gpc - 1) / gpc);
         path_steps += (double)R * (double)nn * (double)(nfine(l) + (l ? nfine(l) / M : 0));
+        normals += (double)R * (double)nn * (double)D;
         return x;
     }
 
@@ -411,7 +557,7 @@ struct BookRunner {
         size_t k = 0;
         for (int c = 0; c < kBookClasses; c++) {
             h[2 + c] = chunk;
-            h[6 + c] = (int)k;
+            h[7 + c] = (int)k;
             for (; k < sp.size() && book_class(opts[sp[k].opt].n_assets) == c; k++) {
                 sp[k].chunk0 = chunk;
                 MCQ_REQUIRE((long long)chunk + (long long)R * sp[k].cpr < INT_MAX, MCQ_ERR_RANGE, "book: chunk count overflow");
@@ -420,8 +566,8 @@ struct BookRunner {
             }
         }
         h[0] = (int)sp.size();
-        h[1] = h[5] = chunk;
-        h[9] = (int)sp.size();
+        h[1] = h[2 + kBookClasses] = chunk;
+        h[7 + kBookClasses] = (int)sp.size();
         s.specs.ensure(sizeof(BookSpec) * std::max<size_t>(max_specs, 1));
         s.hdr.ensure(sizeof(int) * kHdrInts);
         s.out.ensure(sizeof(double) * kBookOut * std::max<size_t>(max_specs, 1));
@@ -432,7 +578,7 @@ struct BookRunner {
     }
 
     static int grid_of(int cls) {
-        static int per_sm[kBookClasses] = {-1, -1, -1};
+        static int per_sm[kBookClasses] = {-1, -1, -1, -1};
         if (per_sm[cls] < 0) {
             const void* fn = (const void*)book_fn(cls);
             MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)book_smem()));
@@ -458,13 +604,16 @@ struct BookRunner {
         Engine& E = engine();
         Slot s;
         s.stream = E.ws(0).stream;
-        cudaStream_t side[2] = {E.ws(1).stream, E.ws(2).stream};
-        cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+        constexpr int kSide = kBookClasses - 1;   // class 0 runs on the main stream
+        cudaStream_t side[kSide];
+        cudaEvent_t fork = nullptr, join[kSide] = {};
+        for (int c = 0; c < kSide; c++) side[c] = E.ws(1 + c).stream;
         MCQ_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
         for (auto& e : join) MCQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         cudaGraphExec_t exec = nullptr;
         const void* captured_records = nullptr;
-        const int grid[kBookClasses] = {grid_of(0), grid_of(1), grid_of(2)};
+        int grid[kBookClasses];
+        for (int c = 0; c < kBookClasses; c++) grid[c] = grid_of(c);
         std::vector<BookSpec> sp;
         auto cleanup = [&]() {
             if (exec) cudaGraphExecDestroy(exec);
@@ -489,11 +638,10 @@ struct BookRunner {
                     cudaGraph_t g = nullptr;
                     MCQ_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
                     MCQ_CUDA(cudaEventRecord(fork, s.stream));
-                    for (int c = 0; c < 2; c++) MCQ_CUDA(cudaStreamWaitEvent(side[c], fork, 0));
+                    for (int c = 0; c < kSide; c++) MCQ_CUDA(cudaStreamWaitEvent(side[c], fork, 0));
+                    for (int c = kBookClasses - 1; c >= 1; c--) launch_book(c, a, grid[c], side[c - 1]);
                     launch_book(0, a, grid[0], s.stream);
-                    launch_book(1, a, grid[1], side[0]);
-                    launch_book(2, a, grid[2], side[1]);
-                    for (int c = 0; c < 2; c++) {
+                    for (int c = 0; c < kSide; c++) {
                         MCQ_CUDA(cudaEventRecord(join[c], side[c]));
                         MCQ_CUDA(cudaStreamWaitEvent(s.stream, join[c], 0));
                     }
@@ -639,6 +787,7 @@ void book_price(const mcq_book_option* opts, int n, const mcq_mlmc_cfg& ml, cons
         stats->time_s = std::chrono::duration<double>(t2 - t1).count();
         stats->setup_s = std::chrono::duration<double>(t1 - t0).count();
         stats->path_steps = b.path_steps;
+        stats->normals = b.normals;
         stats->rounds = (int)b.rounds;
         stats->launches = (int)b.launches;
     }

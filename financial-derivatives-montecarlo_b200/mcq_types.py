@@ -84,7 +84,7 @@ class BookResult(C.Structure):
 
 class BookStats(C.Structure):
     _fields_ = [("time_s", C.c_double), ("setup_s", C.c_double), ("path_steps", C.c_double),
-                ("rounds", C.c_int32), ("launches", C.c_int32)]
+                ("normals", C.c_double), ("rounds", C.c_int32), ("launches", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -178,6 +178,7 @@ typedef struct mcq_book_stats {
     double  time_s;               /* pricing time, after the per-book set-up */
     double  setup_s;              /* parameter upload and scrambled tables */
     double  path_steps;           /* sum over slices of R x points x (fine + coarse steps) */
+    double  normals;              /* sum over slices of R x points x fine steps x assets */
     int32_t rounds;               /* adaptive rounds (batched) / per-option steps (plain) */
     int32_t launches;             /* kernel launches issued */
 } mcq_book_stats;
