@@ -136,19 +136,34 @@ def book_bench(eng, n):
     of the 4096-option synthetic book (d ~ U{1..16}, correlated GBM, Dirichlet weights, T ~
     U[0.1, 3], 16-512 finest steps, eps ~ U[5e-4, 5e-3]), each priced by MLQMC (R = 16, M = 2)
     with its per-asset pathwise deltas.  Each mode is timed by the library around its pricing
-    loop (host wall time with the device synchronised), after a warm-up book."""
-    book = eng.config5_book(n=4096, seed=5)[:n]
-    eng.book_price(book[:8], eng.BOOK_BATCHED)
-    eng.book_price(book[:8], eng.BOOK_PLAIN)
+    loop (host wall time with the device synchronised), after a warm-up book.  Under torchrun
+    the options are dealt round-robin over the ranks (the same n in total) and the time is the
+    maximum over ranks."""
+    import torch
+    rank, _, world = dist_env()
+    full = eng.config5_book(n=4096, seed=5)[:n]
+    mine = [full[i] for i in range(rank, n, world)]
+    eng.book_price(full[:8], eng.BOOK_BATCHED)
+    eng.book_price(full[:8], eng.BOOK_PLAIN)
     out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5); "
-                                     "MLQMC R=16 M=2 n0=1, per-option eps, price + per-asset delta" % n}
+                                     "MLQMC R=16 M=2 n0=1, per-option eps, price + per-asset delta" % n,
+           "sharding": "options round-robin over %d rank(s), fixed total" % world}
     res = {}
     for name, mode in (("batched", eng.BOOK_BATCHED), ("plain", eng.BOOK_PLAIN)):
-        r, st = eng.book_price(book, mode)
+        r, st = eng.book_price(mine, mode) if mine else ([], {"time_s": 0.0, "rounds": 0, "launches": 0,
+                                                               "normals": 0.0, "path_steps": 0.0})
         res[name] = r
-        out[name] = {"options_per_s": n / st["time_s"], "time_s": st["time_s"], "rounds": st["rounds"],
-                     "launches": st["launches"], "normals_per_s": st["normals"] / st["time_s"],
-                     "path_steps_per_s": st["path_steps"] / st["time_s"]}
+        agg = torch.tensor([st["time_s"], st["normals"], st["path_steps"]], dtype=torch.float64, device="cuda")
+        if world > 1:
+            t = agg[:1].clone()
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            w = agg[1:].clone()
+            torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+            agg = torch.cat([t, w])
+        tmax, normals, psteps = agg.tolist()
+        out[name] = {"options_per_s": n / tmax, "time_s": tmax, "rounds": st["rounds"],
+                     "launches": st["launches"], "normals_per_s": normals / tmax,
+                     "path_steps_per_s": psteps / tmax}
     out["batched_over_plain"] = out["batched"]["options_per_s"] / out["plain"]["options_per_s"]
     out["bit_identical"] = all(a["price"] == b["price"] and bool((a["delta"] == b["delta"]).all())
                                for a, b in zip(res["batched"], res["plain"]))
