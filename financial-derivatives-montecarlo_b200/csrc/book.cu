@@ -308,7 +308,9 @@ __global__ void k_book_fin(const __grid_constant__ BookArgs a) {
         double* o = a.out + (size_t)s * kBookOut;
         if (lane == 0) {
             double v = 0.0;
-            for (int r = 0; r < a.R; r++) v += (rep[r] - m) * (rep[r] - m);
+            // separate roundings (no fused multiply-add), so that a host restatement in IEEE
+            // double gives the same bits
+            for (int r = 0; r < a.R; r++) v = __dadd_rn(v, __dmul_rn(rep[r] - m, rep[r] - m));
             o[0] = m;
             o[1] = a.R > 1 ? v / (a.R - 1) : 0.0;
         } else {
