@@ -171,6 +171,38 @@ def book_bench(eng, n):
     return out
 
 
+def book_slice(spec):
+    """One (option, level) slice through the book kernel: a D-asset correlated basket call
+    (seeded as the synthetic book), all 16 replicas, POINTS points (default: about 4e9 normals)."""
+    import numpy as np
+    import torch
+    parts = [int(v) for v in spec.split(":")]
+    d, level = parts[0], parts[1]
+    nf = 2 ** level
+    n = parts[2] if len(parts) > 2 else min(max(1 << 12, int(4e9 / (16 * nf * d))), 1 << 30)
+    eng = load_engine()
+    eng.init(0)
+    rng = np.random.default_rng(3)
+    S0, sig = 100 * rng.uniform(0.8, 1.2, d), rng.uniform(0.1, 0.5, d)
+    A = rng.normal(size=(d, d))
+    Cm = A @ A.T + 0.5 * np.eye(d)
+    dg = np.sqrt(np.diag(Cm))
+    w = rng.dirichlet(np.ones(d))
+    o = eng.book_option(S0, sig, float(w @ S0), 0.03, 1.0, 1e-3, max(level, 2), weights=w,
+                        L=np.linalg.cholesky(Cm / np.outer(dg, dg)))
+    ml, qc = eng.mlmc_cfg(M=2, n0_steps=1), eng.qmc_cfg(R=16)
+    eng.book_level_sums(o, level, 0, min(n, 4096), ml, qc)
+    best = float("inf")
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.book_level_sums(o, level, 0, n, ml, qc)
+        best = min(best, time.perf_counter() - t0)
+    normals = 16.0 * n * nf * d
+    print(json.dumps({"book_slice": {"assets": d, "level": level, "points": n, "replicas": 16,
+                                     "normals": normals, "seconds": best, "normals_per_s": normals / best}}))
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
@@ -207,10 +239,15 @@ def main():
     ap.add_argument("--no-variants", action="store_true", help="skip the bridge / PCA orderings")
     ap.add_argument("--book-options", type=int, default=64,
                     help="options of the synthetic basket book priced batched and plain (0: skip)")
+    ap.add_argument("--book-slice", default=None, metavar="D:LEVEL[:POINTS]",
+                    help="only price one slice of a D-asset basket at LEVEL through the book kernel "
+                         "(R = 16, M = 2, n0 = 1) and print its normals/s: the profiling case")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.book_slice:
+        return book_slice(args.book_slice)
 
     import torch
     rank, local_rank, world = dist_env()

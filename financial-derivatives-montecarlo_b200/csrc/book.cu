@@ -74,9 +74,9 @@ struct BookArgs {
 __host__ __device__ inline int book_class(int d) { return (d - 1) >> 2; }
 
 // Per-warp shared memory: the 32 x 32 transpose tile, the option's Cholesky factor with rows
-// padded to a multiple of 4 floats, and the FP64 record of the chunk.
+// padded to a multiple of 4 floats, its volatilities, and the FP64 record of the chunk.
 constexpr int kBookLsFloats = kMaxBasket * kMaxBasket;
-constexpr int kBookWarpFloats = 1024 + kBookLsFloats + 2 * kBookNST;
+constexpr int kBookWarpFloats = 1024 + kBookLsFloats + kMaxBasket + 2 * kBookNST;
 
 // The coupled basket pair of one path for a basket of exactly D assets: the correlated Euler
 // step S + S (mu h + sigma dW) with dW = L x, x = z sqrt(h), coarse steps on the summed fine
@@ -97,7 +97,7 @@ struct BookPath {
         m = 0;
     }
     // x: this step's D normals times sqrt(h); L4: lower Cholesky rows padded to DP floats
-    __device__ __forceinline__ void step(const float (&x)[D], const float4* L4, const float (&sg)[D], float muh_f,
+    __device__ __forceinline__ void step(const float (&x)[D], const float4* L4, const float* sg, float muh_f,
                                          float muh_c, int Mc) {
 #pragma unroll
         for (int q = 0; q < D; q++) {
@@ -175,9 +175,8 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
         Ls[i] = (col <= row) ? __ldg(bk + 3 * D + row * D + col) : 0.f;
     }
     if (lane < NS) wrec[lane] = 0.0;
-    float sg[D];
-#pragma unroll
-    for (int q = 0; q < D; q++) sg[q] = __ldg(bk + D + q);
+    float* sg = Ls + kBookLsFloats;   // volatilities, read from shared memory at every step
+    if (lane < D) sg[lane] = __ldg(bk + D + lane);
     int nf = a.n0;
     for (int l = 0; l < s.level; l++) nf *= a.M;
     const int nc = s.level ? nf / a.M : 0;
@@ -224,18 +223,24 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
                 const int dim = k0 * D + lane;
                 sobol_tile(dr, dstride, dim, lane < W && dim < Dt, g, a.u_cap, buf, lane);
                 __syncwarp();
-                float z[32];
-                read_row(buf, lane, z);
-                __syncwarp();
+                // this path's row of the tile, read per step as float4 chunks (conflict-free in
+                // the swizzled layout) so that only one step's normals are live in registers
+                const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
 #pragma unroll
                 for (int st = 0; st < S; st++) {
                     if (k0 + st < nf) {
                         float x[D];
 #pragma unroll
-                        for (int c = 0; c < D; c++) x[c] = z[st * D + c] * sqrt_h;
+                        for (int c = 0; c < D; c++) {
+                            const int col = st * D + c;
+                            const float4 v = row4[(col >> 2) ^ (lane & 7)];
+                            const float zc = (col & 3) == 0 ? v.x : (col & 3) == 1 ? v.y : (col & 3) == 2 ? v.z : v.w;
+                            x[c] = zc * sqrt_h;
+                        }
                         path.step(x, L4, sg, muh_f, muh_c, Mc);
                     }
                 }
+                __syncwarp();
             }
             float y[NS];
             path.finish(bk, K, disc, has_c, y);
@@ -256,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     float* buf = reinterpret_cast<float*>(smem4) + wib * kBookWarpFloats;
     float* Ls = buf + 1024;
-    double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats);
+    double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats + kMaxBasket);
     const int c_end = a.hdr[3 + CLS];
     const int s_beg = a.hdr[7 + CLS], s_last = a.hdr[8 + CLS] - 1;
     for (;;) {
