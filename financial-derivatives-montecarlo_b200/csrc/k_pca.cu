@@ -127,14 +127,20 @@ __device__ __forceinline__ void sobol_tile_to_A(const uint32_t* __restrict__ dr,
     }
     unsigned char* base = A + (e & 7) * 2;
     const int chunk = e >> 3;
+    // four blocks of eight points, the block loop rolled (the gray-code steps as in sobol_tile)
+#pragma unroll 1
+    for (int b = 0; b < 4; b++) {
 #pragma unroll
-    for (int i = 0; i < 32; i++) {
-        const int r = row0 + i;
-        *reinterpret_cast<__half*>(base + r * 128 + ((chunk ^ (r & 7)) << 4)) =
-            __float2half_rn(sobol_normal(x, u_cap));
-        if (i < 31) {
-            const int c = cx_ctz(i + 1);
-            x ^= (c == 0) ? L0 : (c == 1) ? L1 : (c == 2) ? L2 : (c == 3) ? L3 : L4;
+        for (int i = 0; i < 8; i++) {
+            const int r = row0 + 8 * b + i;
+            *reinterpret_cast<__half*>(base + r * 128 + ((chunk ^ (r & 7)) << 4)) =
+                __float2half_rn(sobol_normal(x, u_cap));
+            if (i < 7) {
+                const int c = cx_ctz(i + 1);
+                x ^= (c == 0) ? L0 : (c == 1) ? L1 : L2;
+            } else if (b < 3) {
+                x ^= (b == 1) ? L4 : L3;
+            }
         }
     }
 }
