@@ -141,10 +141,13 @@ def book_bench(eng, n):
     maximum over ranks."""
     import torch
     rank, _, world = dist_env()
-    full = eng.config5_book(n=4096, seed=5)[:n]
+    book = eng.config5_book(n=4096, seed=5)
+    full = book[:n]
     mine = [full[i] for i in range(rank, n, world)]
-    eng.book_price(full[:8], eng.BOOK_BATCHED)
-    eng.book_price(full[:8], eng.BOOK_PLAIN)
+    # warm-up: one option of every basket width (all kernels loaded, graphs and streams set up)
+    warm = [next(o for o in book if o.n_assets == d) for d in range(1, 17)]
+    eng.book_price(warm, eng.BOOK_BATCHED)
+    eng.book_price(warm, eng.BOOK_PLAIN)
     out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5); "
                                      "MLQMC R=16 M=2 n0=1, per-option eps, price + per-asset delta" % n,
            "sharding": "options round-robin over %d rank(s), fixed total" % world}

@@ -552,10 +552,12 @@ struct BookRunner {
         return x;
     }
 
-    // Order slices by width class, assign chunk ranges, upload slices and header on s.stream.
+    // Order slices by basket width, assign chunk ranges, upload slices and header on s.stream.
     int upload(Slot& s, std::vector<BookSpec>& sp) {
+        // by basket width: a class kernel's warps then take chunks of one width at a time, so one
+        // specialisation's code is hot in the instruction cache instead of four
         std::stable_sort(sp.begin(), sp.end(), [&](const BookSpec& a, const BookSpec& b) {
-            return book_class(opts[a.opt].n_assets) < book_class(opts[b.opt].n_assets);
+            return opts[a.opt].n_assets < opts[b.opt].n_assets;
         });
         int* h = (int*)s.hspecs.ensure(sizeof(int) * kHdrInts + sizeof(BookSpec) * std::max<size_t>(sp.size(), 1));
         std::memset(h, 0, sizeof(int) * kHdrInts);
