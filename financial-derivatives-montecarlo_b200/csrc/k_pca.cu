@@ -3,15 +3,17 @@
 // The reference applies PCA as three HBM passes: cast the normals to fp16, one cuBLAS GEMM
 // dW = Z M^T over the whole [D x N] array, then the path kernel (methods_cuda.cu:1150-1166,
 // :1228-1229, :720-724).  Here one kernel does it per tile of 256 paths:
-//   1. eight warps generate the scrambled-Sobol normals of their 32 paths, 64 dimensions at a
-//      time, and store them as fp16 (round to nearest, as __float2half in the reference)
-//      straight into a 128-byte-swizzled K-major shared-memory tile (two buffers);
+//   1. sixteen warps generate the scrambled-Sobol normals of the tile's paths, 64 dimensions at
+//      a time (warps w and w + 8 make the two 32-dimension halves of the rows of paths 32(w mod 8)
+//      .. 32(w mod 8) + 31), and store them as fp16 (round to nearest, as __float2half in the
+//      reference) straight into a 128-byte-swizzled K-major shared-memory tile (two buffers);
 //   2. one elected thread issues tcgen05.mma kind::f16 (fp16 x fp16 -> fp32) for the two
 //      128-row halves against the PCA factor M (fp16, resident in shared memory for the whole
 //      kernel), accumulating dW in tensor memory; tcgen05.commit signals an mbarrier;
-//   3. each warp drains the TMEM lanes of its 32 paths with tcgen05.ld (32 columns = 32 time
-//      steps at a time) and feeds the increments to the path consumer.
-// Generation of K-block kb+1 overlaps the MMA of K-block kb.  Every mbarrier wait is bounded:
+//   3. warps 0-7 drain the TMEM lanes of their 32 paths with tcgen05.ld (32 columns = 32 time
+//      steps at a time) and feed the increments to the path consumer.
+// Generation of K-block kb+1 overlaps the MMA of K-block kb, and warps 8-15 generate the next
+// tile's first K-block while warps 0-7 drain this one.  Every mbarrier wait is bounded:
 // after the limit the CTA records MCQ_ERR_TIMEOUT in p.err, frees its TMEM and returns.
 //
 // Supported sizes: N = D in {64, 128, 256} (K-blocks of 64, MMA N <= 256).
@@ -22,8 +24,9 @@
 
 namespace mcq {
 
-constexpr int kPcaWarps = 8;
-constexpr int kPcaThreads = kPcaWarps * 32;
+constexpr int kPcaWarps = 8;                     // path-owning warps: 32 paths each, 256 per tile
+constexpr int kPcaGenWarps = 2 * kPcaWarps;       // all warps generate, half a K-block each
+constexpr int kPcaThreads = kPcaGenWarps * 32;
 constexpr int kABufBytes = 256 * 128;        // 256 rows x 64 fp16
 constexpr uint32_t kWaitLimit = 1u << 26;    // polls of an mbarrier before giving up
 
@@ -201,8 +204,9 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
         Acc<C::NST> acc;
         acc.zero();
         for (int t = t_beg; t < t_end && !failed; t++) {
-            const uint64_t h = p.g0 + (uint64_t)t * 8 + (uint64_t)warp;
+            const uint64_t h = p.g0 + (uint64_t)t * 8 + (uint64_t)(warp & 7);
             const uint64_t n = h * 32 + (uint64_t)lane;
+            const int khalf = warp >> 3;   // which 32 of the K-block's 64 dimensions this warp makes
             bool outstanding[2] = {false, false};
             for (int kb = 0; kb < nkb; kb++) {
                 const int b = kb & 1;
@@ -213,8 +217,7 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
                     outstanding[b] = false;
                     if (__syncthreads_or(!ok)) { failed = true; break; }
                 }
-                sobol_tile_to_A(dr, N, kb * 64 + lane, h, p.u_cap, A, warp * 32, lane);
-                sobol_tile_to_A(dr, N, kb * 64 + 32 + lane, h, p.u_cap, A, warp * 32, 32 + lane);
+                sobol_tile_to_A(dr, N, kb * 64 + 32 * khalf + lane, h, p.u_cap, A, (warp & 7) * 32, 32 * khalf + lane);
                 fence_proxy_async();
                 __syncthreads();
                 if (tid == 0) {
@@ -243,6 +246,10 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
             }
             if (__syncthreads_or(!ok)) { failed = true; break; }
             tc_fence_after();
+            if (warp >= kPcaWarps) {   // generators only: go on to the next tile's first K-block
+                tc_fence_before();
+                continue;
+            }
             C cons;
             cons.init(p);
             if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
@@ -260,7 +267,7 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
             if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
             tc_fence_before();   // TMEM reads done before the next tile's first MMA overwrites it
         }
-        acc.flush(p.partials + ((size_t)item * kPcaWarps + warp) * C::NST, lane);
+        if (warp < kPcaWarps) acc.flush(p.partials + ((size_t)item * kPcaWarps + warp) * C::NST, lane);
     }
     if (failed && tid == 0) atomicExch(p.err, MCQ_ERR_TIMEOUT_CODE);
     tc_fence_before();
