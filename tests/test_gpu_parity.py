@@ -160,3 +160,19 @@ def test_launch_variants_are_bit_identical(gpu, model, pay):
     finally:
         os.environ.pop("MCQ_TUNE", None)
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("dupire", "eur")])
+def test_bridge_launch_variants_are_bit_identical(gpu, model, pay):
+    import os
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    bb = gpu.bb_create(256, m.T)
+    out = []
+    try:
+        for v in ("0", "1"):
+            os.environ["MCQ_TUNE"] = v
+            out.append(gpu.qmc_pass(m, p, 256, noise=gpu.BB, bb=bb, salt_base=42, R=4, offset=3, n_points=20000))
+    finally:
+        os.environ.pop("MCQ_TUNE", None)
+        bb.close()
+    assert np.array_equal(out[0], out[1])
