@@ -143,17 +143,64 @@ struct BookPath {
     }
 };
 
-// Warp sum of one path's statistics into the chunk's FP64 record (lane 0 adds).
-template <int NS>
-__device__ __forceinline__ void book_acc(const float (&y)[NS], bool valid, double* wrec, int lane) {
+// Chunk accumulator of the per-path statistics.  Narrow baskets (NS <= 12) keep FP64 sums per
+// lane and reduce across the warp once per chunk: their paths are short, and a warp reduction
+// per path would cost as much as the path.  Wider ones add each path's warp sum (FP32 shuffle
+// tree) to an FP64 record in shared memory, keeping their registers for the path state.
+template <int NS, bool LANE = (NS <= 12)>
+struct BookAcc {
+    double v[LANE ? NS : 1];
+    double* wrec;
+    __device__ __forceinline__ void init(double* w, int lane) {
+        wrec = w;
+        if constexpr (LANE) {
 #pragma unroll
-    for (int q = 0; q < NS; q++) {
-        float v = valid ? y[q] : 0.f;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (lane == 0) wrec[q] += (double)v;
+            for (int q = 0; q < NS; q++) v[q] = 0.0;
+        } else {
+            if (lane < NS) wrec[lane] = 0.0;
+            __syncwarp();
+        }
     }
-}
+    __device__ __forceinline__ void add(const float (&y)[NS], bool valid, int lane) {
+        if constexpr (LANE) {
+            if (valid) {
+#pragma unroll
+                for (int q = 0; q < NS; q++) v[q] += (double)y[q];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < NS; q++) {
+                float t = valid ? y[q] : 0.f;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+                if (lane == 0) wrec[q] += (double)t;
+            }
+        }
+    }
+    // writes the chunk record [kBookNST] (zeros past NS)
+    __device__ __forceinline__ void flush(double* rec, int lane) {
+        if constexpr (LANE) {
+#pragma unroll
+            for (int q = 0; q < NS; q++) {
+                double t = v[q];
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+                v[q] = t;
+            }
+            if (lane < kBookNST) {
+                double out = 0.0;
+#pragma unroll
+                for (int q = 0; q < NS; q++)
+                    if (lane == q) out = v[q];
+                rec[lane] = out;
+            }
+        } else {
+            __syncwarp();
+            if (lane < kBookNST) rec[lane] = (lane < NS) ? wrec[lane] : 0.0;
+        }
+        __syncwarp();
+    }
+};
 
 // One chunk of a slice for a basket of exactly D assets: groups [gb, ge) of replica r.
 //
@@ -174,7 +221,8 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
         const int row = i / DP, col = i - row * DP;
         Ls[i] = (col <= row) ? __ldg(bk + 3 * D + row * D + col) : 0.f;
     }
-    if (lane < NS) wrec[lane] = 0.0;
+    BookAcc<NS> acc;
+    acc.init(wrec, lane);
     float* sg = Ls + kBookLsFloats;   // volatilities, read from shared memory at every step
     if (lane < D) sg[lane] = __ldg(bk + D + lane);
     int nf = a.n0;
@@ -211,7 +259,7 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
                 float y[NS];
                 path.finish(bk, K, disc, has_c, y);
                 const uint64_t n = (g + q) * 32 + (uint64_t)lane;
-                book_acc<NS>(y, n >= s.offset && n < pend, wrec, lane);
+                acc.add(y, n >= s.offset && n < pend, lane);
             }
             __syncwarp();
         }
@@ -245,12 +293,10 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
             float y[NS];
             path.finish(bk, K, disc, has_c, y);
             const uint64_t n = g * 32 + (uint64_t)lane;
-            book_acc<NS>(y, n >= s.offset && n < pend, wrec, lane);
+            acc.add(y, n >= s.offset && n < pend, lane);
         }
     }
-    __syncwarp();
-    if (lane < kBookNST) rec[lane] = (lane < NS) ? wrec[lane] : 0.0;
-    __syncwarp();
+    acc.flush(rec, lane);
 }
 
 // Persistent work-queue kernel of one width class: warps take chunks from the class's atomic
