@@ -40,6 +40,7 @@ constexpr int kBookMaxLevels = 12;
 constexpr int kBookMaxR = 32;
 constexpr int kBookClasses = 4;            // basket width 1-4, 5-8, 9-12, 13-16
 constexpr int kChunkNormals = 8192;        // normals per lane a chunk aims at
+constexpr int kMinChunksPerRep = 64;
 constexpr int kMaxChunksPerRep = 256;
 
 // hdr (int32): [0] n_specs, [1] n_chunks, [2 + c] first chunk of class c, [6] = n_chunks,
@@ -418,11 +419,20 @@ struct OptState {
     long long pend_n[kBookMaxLevels];
 };
 
-// Device and pinned buffers of one launch context (the batched round, or one level stream).
+// Grow-only with doubling, so that a book's rounds reallocate (and the batched graph is
+// re-captured) a logarithmic number of times.
+inline void* grow(DevBuf& b, size_t bytes) { return b.ensure(bytes <= b.cap ? bytes : std::max(bytes, 2 * b.cap)); }
+
+// Device and pinned buffers of one launch context (the batched round, or one level stream):
+// the engine workspace's long-lived scratch, so that a book allocates only when it needs more
+// than an earlier one (an allocation or free would synchronise the device inside the run).
 struct Slot {
-    cudaStream_t stream = nullptr;
-    DevBuf specs, hdr, records, out;
-    PinnedBuf hspecs, hout;
+    cudaStream_t stream;
+    DevBuf &specs, &hdr, &records, &out;
+    PinnedBuf &hspecs, &hout;
+    explicit Slot(Workspace& w)
+        : stream(w.stream), specs(w.xbuf[0]), hdr(w.xbuf[1]), records(w.xbuf[2]), out(w.xbuf[3]),
+          hspecs(w.xpin[0]), hout(w.xpin[1]) {}
 };
 
 }  // namespace
@@ -433,8 +443,9 @@ struct BookRunner {
     mcq_mlmc_cfg ml{};
     mcq_qmc_cfg qc{};
     int R = 0, M = 0, n0 = 0, max_L_all = 2;
-    DevBuf d_opts, d_bdata;
-    std::vector<DevBuf> dirs;
+    DevBuf* d_opts = nullptr;     // engine scratch (workspace 0)
+    DevBuf* d_bdata = nullptr;
+    std::vector<DevBuf*> dirs;    // level l's table in workspace 1 + l
     std::vector<int> dstride;
     std::vector<OptState> st;
     size_t max_specs = 0;
@@ -452,10 +463,10 @@ struct BookRunner {
         std::memset(&a, 0, sizeof(a));
         a.hdr = (int*)s.hdr.p;
         a.specs = (const BookSpec*)s.specs.p;
-        a.opts = (const BookOptDev*)d_opts.p;
-        a.bdata = (const float*)d_bdata.p;
+        a.opts = (const BookOptDev*)d_opts->p;
+        a.bdata = (const float*)d_bdata->p;
         for (int l = 0; l <= max_L_all; l++) {
-            a.dirs[l] = (const uint32_t*)dirs[l].p;
+            a.dirs[l] = (const uint32_t*)dirs[l]->p;
             a.dstride[l] = dstride[l];
         }
         a.R = R; a.M = M; a.n0 = n0;
@@ -486,22 +497,31 @@ struct BookRunner {
             dmax = std::max(dmax, d);
         }
         cudaStream_t s0 = E.ws(0).stream;
-        MCQ_CUDA(cudaMemcpyAsync(d_opts.ensure(sizeof(BookOptDev) * n), ho.data(), sizeof(BookOptDev) * n,
+        d_opts = &E.ws(0).xbuf[5];
+        d_bdata = &E.ws(0).xbuf[6];
+        MCQ_CUDA(cudaMemcpyAsync(grow(*d_opts, sizeof(BookOptDev) * n), ho.data(), sizeof(BookOptDev) * n,
                                  cudaMemcpyHostToDevice, s0));
-        MCQ_CUDA(cudaMemcpyAsync(d_bdata.ensure(sizeof(float) * bd.size()), bd.data(), sizeof(float) * bd.size(),
+        MCQ_CUDA(cudaMemcpyAsync(grow(*d_bdata, sizeof(float) * bd.size()), bd.data(), sizeof(float) * bd.size(),
                                  cudaMemcpyHostToDevice, s0));
         // one scrambled table per level shared by all options; an option of d assets uses its
         // first nfine(l) d dimensions, exactly the table run_mlqmc builds for it
-        dirs.resize(max_L_all + 1);
+        dirs.assign(max_L_all + 1, nullptr);
         dstride.assign(max_L_all + 1, 0);
         for (int l = 0; l <= max_L_all; l++) {
             dstride[l] = (int)(dmax * nfine(l));
-            uint32_t* t = (uint32_t*)dirs[l].ensure(sizeof(uint32_t) * (size_t)R * 33 * dstride[l]);
+            dirs[l] = &E.ws(1 + l).xbuf[4];
+            uint32_t* t = (uint32_t*)grow(*dirs[l], sizeof(uint32_t) * (size_t)R * 33 * dstride[l]);
             launch_prescramble(E.d_dv, qc.salt_base + (uint32_t)(l * R), R, dstride[l], t, s0);
         }
         MCQ_CUDA(cudaStreamSynchronize(s0));
         max_specs = (size_t)n * (max_L_all + 1);
         st.assign(n, OptState());
+        // chunk records reserved before the timed run (an allocation here can take 0.1 s): the
+        // batched rounds' typical need (every slice split kMinChunksPerRep ways), at most 1 GiB,
+        // and one slice's worst case per level stream
+        const size_t rec = sizeof(double) * kBookNST;
+        grow(E.ws(0).xbuf[2], std::min<size_t>(max_specs * (size_t)R * kMinChunksPerRep * rec, (size_t)1 << 30));
+        for (int l = 0; l <= max_L_all; l++) grow(E.ws(1 + l).xbuf[2], (size_t)R * kMaxChunksPerRep * rec);
     }
 
     // The next slices option i needs (run_mlqmc_cuda :1950-2000); steps that need no sample
@@ -585,11 +605,13 @@ struct BookRunner {
         x.level = l;
         x.offset = (uint32_t)s.next_off[l];
         x.n_points = (uint32_t)nn;
-        // chunk size from the slice alone: about kChunkNormals normals per lane, at most
-        // kMaxChunksPerRep chunks per replica
+        // chunk size from the slice alone: at most kChunkNormals normals per lane, split into
+        // at least kMinChunksPerRep chunks per replica where the slice has that many groups (a
+        // round whose few slices are small still spreads over the GPU), at most kMaxChunksPerRep
         const long long D = (long long)opts[i].n_assets * nfine(l);
         const uint64_t G = ((uint64_t)x.offset + x.n_points - 1) / 32 + 1 - (x.offset >> 5);
-        uint64_t gpc = (uint64_t)std::max<long long>(1, kChunkNormals / D);
+        uint64_t gpc = std::min<uint64_t>((uint64_t)std::max<long long>(1, kChunkNormals / D),
+                                          std::max<uint64_t>(1, G / kMinChunksPerRep));
         gpc = std::max<uint64_t>(gpc, (G + kMaxChunksPerRep - 1) / kMaxChunksPerRep);
         x.gpc = (int)gpc;
         x.cpr = (int)((G + gpc - 1) / gpc);
@@ -605,7 +627,7 @@ struct BookRunner {
         std::stable_sort(sp.begin(), sp.end(), [&](const BookSpec& a, const BookSpec& b) {
             return opts[a.opt].n_assets < opts[b.opt].n_assets;
         });
-        int* h = (int*)s.hspecs.ensure(sizeof(int) * kHdrInts + sizeof(BookSpec) * std::max<size_t>(sp.size(), 1));
+        int* h = (int*)s.hspecs.ensure(sizeof(int) * kHdrInts + sizeof(BookSpec) * std::max<size_t>(max_specs, 1));
         std::memset(h, 0, sizeof(int) * kHdrInts);
         BookSpec* hs = reinterpret_cast<BookSpec*>(h + kHdrInts);
         int chunk = 0;
@@ -657,8 +679,7 @@ struct BookRunner {
     // ---- batched: one graph per book, replayed once per round
     void run_batched() {
         Engine& E = engine();
-        Slot s;
-        s.stream = E.ws(0).stream;
+        Slot s(E.ws(0));
         constexpr int kSide = kBookClasses - 1;   // class 0 runs on the main stream
         cudaStream_t side[kSide];
         cudaEvent_t fork = nullptr, join[kSide] = {};
@@ -685,7 +706,7 @@ struct BookRunner {
                 if (sp.empty()) break;
                 long long chunks = 0;
                 for (auto& x : sp) chunks += (long long)R * x.cpr;
-                s.records.ensure(sizeof(double) * kBookNST * (size_t)std::max<long long>(chunks, 1));
+                grow(s.records, sizeof(double) * kBookNST * (size_t)std::max<long long>(chunks, 1));
                 upload(s, sp);
                 if (!exec || captured_records != s.records.p) {   // (re)capture when a buffer moved
                     if (exec) { MCQ_CUDA(cudaGraphExecDestroy(exec)); exec = nullptr; }
@@ -708,7 +729,7 @@ struct BookRunner {
                     captured_records = s.records.p;
                 }
                 MCQ_CUDA(cudaGraphLaunch(exec, s.stream));
-                double* ho = (double*)s.hout.ensure(sizeof(double) * kBookOut * sp.size());
+                double* ho = (double*)s.hout.ensure(sizeof(double) * kBookOut * std::max<size_t>(max_specs, 1));
                 MCQ_CUDA(cudaMemcpyAsync(ho, s.out.p, sizeof(double) * kBookOut * sp.size(), cudaMemcpyDeviceToHost,
                                          s.stream));
                 MCQ_CUDA(cudaStreamSynchronize(s.stream));
@@ -729,8 +750,9 @@ struct BookRunner {
     // ---- plain: per option, one launch of the option's class kernel per level on its stream
     void run_plain() {
         Engine& E = engine();
-        std::vector<Slot> slots(max_L_all + 1);
-        for (int l = 0; l <= max_L_all; l++) slots[l].stream = E.ws(1 + l).stream;
+        std::vector<Slot> slots;
+        slots.reserve(max_L_all + 1);
+        for (int l = 0; l <= max_L_all; l++) slots.emplace_back(E.ws(1 + l));
         std::vector<BookSpec> one(1);
         for (int i = 0; i < n; i++) {
             const int cls = book_class(opts[i].n_assets);
@@ -745,7 +767,7 @@ struct BookRunner {
                     const int l = s.pend_level[k];
                     Slot& sl = slots[l];
                     one[0] = make_spec(i, l, s.pend_n[k]);
-                    sl.records.ensure(sizeof(double) * kBookNST * (size_t)R * one[0].cpr);
+                    grow(sl.records, sizeof(double) * kBookNST * (size_t)R * one[0].cpr);
                     const int chunks = upload(sl, one);
                     const BookArgs a = args(sl);
                     launch_book(cls, a, std::max(1, std::min(grid_of(cls), (chunks + kWarpsPerBlock - 1) / kWarpsPerBlock)),
@@ -799,10 +821,9 @@ void book_level_sums(const mcq_book_option& opt, const mcq_mlmc_cfg& ml, const m
     b.qc = qc;
     b.setup();
     b.st[0].next_off[level] = offset;
-    Slot s;
-    s.stream = engine().ws(0).stream;
+    Slot s(engine().ws(0));
     std::vector<BookSpec> one(1, b.make_spec(0, level, n_points));
-    s.records.ensure(sizeof(double) * kBookNST * (size_t)b.R * one[0].cpr);
+    grow(s.records, sizeof(double) * kBookNST * (size_t)b.R * one[0].cpr);
     const int chunks = b.upload(s, one);
     const int cls = book_class(opt.n_assets);
     b.launch_book(cls, b.args(s), BookRunner::grid_of(cls), s.stream);

@@ -55,6 +55,8 @@ struct Workspace {
     DevBuf partials, sums, dirs, aux, dump, err;
     bool err_armed = false;   // err holds a fresh status from the last tensor-core pass
     PinnedBuf hsums, haux;
+    DevBuf xbuf[8];       // long-lived scratch of the batched book (book.cu): kept across calls
+    PinnedBuf xpin[2];
     uint32_t dirs_salt0 = 0;
     int dirs_R = -1, dirs_D = -1;
     void ensure_stream();
