@@ -352,6 +352,8 @@ def main():
         e2e_t = float(t.item())
     e2e_value = world * e2e_ps / e2e_t
     doublings = max(1, int(round(__import__("math").log2(e2e_last["n_samples"] / (REPS << 14)))) + 1)
+    import ctypes
+    h2d_e2e = ctypes.sizeof(m) + ctypes.sizeof(p) + ctypes.sizeof(cfg)
 
     book = None if args.book_options <= 0 else book_bench(eng, args.book_options)
 
@@ -386,10 +388,12 @@ def main():
                    "l2": "flushed (256 MiB write) between steps; inputs are parameter-sized"},
         "price_check": price,
         "orderings": variants,
-        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 0,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d_e2e,
                 "d2h_bytes_per_step": doublings * REPS * 2 * 8,
-                "what": "mcq_run_qmc (run_qmc_cuda entry) eps=1e-3 from 2^14 pts/replica, host wall time; "
-                        "inputs are host parameter structs (kernel arguments), no array copies",
+                "what": "mcq_run_qmc (run_qmc_cuda entry) eps=1e-3 from 2^14 pts/replica, host wall time; a step "
+                        "is one driver call: its inputs are the host model / payoff / config structs (copied to "
+                        "the device as kernel parameters, counted in h2d), its outputs the per-replica sums of "
+                        "each doubling read back (d2h)",
                 "price": e2e_last["price"], "std_error": e2e_last["std_error"], "n_samples": e2e_last["n_samples"],
                 "path_steps_per_run": e2e_last["path_steps"], "ms_per_run": 1e3 * e2e_t / args.e2e_runs},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
