@@ -28,7 +28,8 @@ EXPORTS = [
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
     "mcq_mc_pass", "mcq_level_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
     "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_qmc_pass_noalloc", "mcq_adjoint",
-    "mcq_book_price", "mcq_book_level_sums",
+    "mcq_book_price", "mcq_book_level_sums", "mcq_book_create", "mcq_book_submit", "mcq_book_size",
+    "mcq_book_run", "mcq_book_clear", "mcq_book_free",
 ]
 
 
@@ -270,6 +271,47 @@ def book_price(options, mode=BOOK_BATCHED, ml=None, qc=None):
         res.append({"price": r.price, "std_error": r.std_error, "delta": np.array(r.delta[:o.n_assets]),
                     "n_samples": r.n_samples, "levels": r.levels, "converged": bool(r.converged)})
     return res, st.as_dict()
+
+
+class Book:
+    """mcq_book: a book built up by submit() and priced by run() (the same pricing as book_price).
+    The library copies the submitted options, so the Python option objects may be dropped."""
+
+    def __init__(self):
+        self.h = C.c_void_p()
+        _check(lib().mcq_book_create(C.byref(self.h)))
+
+    def submit(self, options):
+        arr = (T.BookOption * len(options))(*options)
+        _check(lib().mcq_book_submit(self.h, arr, C.c_int(len(options))))
+
+    def __len__(self):
+        n = C.c_int()
+        _check(lib().mcq_book_size(self.h, C.byref(n)))
+        return n.value
+
+    def run(self, mode=BOOK_BATCHED, ml=None, qc=None):
+        n = len(self)
+        out = (T.BookResult * n)()
+        st = T.BookStats()
+        ml = ml if ml is not None else mlmc_cfg(M=2, n0_steps=1)
+        qc = qc if qc is not None else qmc_cfg(R=16)
+        _check(lib().mcq_book_run(self.h, C.byref(ml), C.byref(qc), C.c_int(mode), out, C.byref(st)))
+        return out, st.as_dict()
+
+    def clear(self):
+        _check(lib().mcq_book_clear(self.h))
+
+    def close(self):
+        if self.h:
+            _check(lib().mcq_book_free(self.h))
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def book_level_sums(option, level, offset=0, n_points=1024, ml=None, qc=None):

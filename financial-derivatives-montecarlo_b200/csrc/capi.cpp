@@ -477,6 +477,85 @@ int mcq_book_price(const mcq_book_option* opts, int n, const mcq_mlmc_cfg* ml, c
     API_END
 }
 
+// Book object: owned copies of the submitted options and their arrays.
+struct mcq_book_s {
+    struct Owned {
+        mcq_book_option o;
+        std::vector<double> S0, sigma, weights, L;
+    };
+    std::vector<Owned> items;
+};
+
+int mcq_book_create(mcq_book* out) {
+    API_BEGIN_NOINIT
+    NEED(out);
+    *out = new mcq_book_s();
+    API_END
+}
+
+int mcq_book_submit(mcq_book b, const mcq_book_option* opts, int n) {
+    API_BEGIN_NOINIT
+    NEED(b); NEED(opts);
+    MCQ_REQUIRE(n >= 0, MCQ_ERR_INVALID, "book: n must be >= 0");
+    std::vector<mcq_book_s::Owned> add((size_t)n);
+    for (int i = 0; i < n; i++) {
+        const mcq_book_option& o = opts[i];
+        MCQ_REQUIRE(o.n_assets >= 1 && o.n_assets <= MCQ_BOOK_MAX_ASSETS, MCQ_ERR_UNSUPPORTED,
+                    "book option " + std::to_string(i) + ": needs 1..16 assets");
+        MCQ_REQUIRE(o.S0 && o.sigma, MCQ_ERR_INVALID, "book option " + std::to_string(i) + ": needs S0 and sigma");
+        const int d = o.n_assets;
+        mcq_book_s::Owned& w = add[(size_t)i];
+        w.o = o;
+        w.S0.assign(o.S0, o.S0 + d);
+        w.sigma.assign(o.sigma, o.sigma + d);
+        if (o.weights) w.weights.assign(o.weights, o.weights + d);
+        if (o.L) w.L.assign(o.L, o.L + (size_t)d * d);
+    }
+    for (auto& w : add) b->items.push_back(std::move(w));
+    for (auto& w : b->items) {   // re-point at the owned arrays (push_back may have moved them)
+        w.o.S0 = w.S0.data();
+        w.o.sigma = w.sigma.data();
+        w.o.weights = w.weights.empty() ? nullptr : w.weights.data();
+        w.o.L = w.L.empty() ? nullptr : w.L.data();
+    }
+    API_END
+}
+
+int mcq_book_size(mcq_book b, int* n) {
+    API_BEGIN_NOINIT
+    NEED(b); NEED(n);
+    *n = (int)b->items.size();
+    API_END
+}
+
+int mcq_book_run(mcq_book b, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc, int mode, mcq_book_result* out,
+                 mcq_book_stats* stats) {
+    API_BEGIN
+    NEED(b); NEED(ml); NEED(qc); NEED(out);
+    MCQ_REQUIRE(!b->items.empty(), MCQ_ERR_INVALID, "book: nothing submitted");
+    MCQ_REQUIRE(mode == MCQ_BOOK_BATCHED || mode == MCQ_BOOK_PLAIN, MCQ_ERR_INVALID, "book: unknown mode");
+    std::vector<mcq_book_option> opts;
+    opts.reserve(b->items.size());
+    for (auto& w : b->items) opts.push_back(w.o);
+    book_validate(opts.data(), (int)opts.size(), *ml, *qc);
+    ensure_ready();
+    book_price(opts.data(), (int)opts.size(), *ml, *qc, mode, out, stats);
+    API_END
+}
+
+int mcq_book_clear(mcq_book b) {
+    API_BEGIN_NOINIT
+    NEED(b);
+    b->items.clear();
+    API_END
+}
+
+int mcq_book_free(mcq_book b) {
+    API_BEGIN_NOINIT
+    delete b;
+    API_END
+}
+
 int mcq_book_level_sums(const mcq_book_option* opt, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc, int level,
                         uint32_t offset, int64_t n_points, double* sums_host) {
     API_BEGIN

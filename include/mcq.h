@@ -266,6 +266,20 @@ int mcq_adjoint(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t s
 int mcq_book_price(const mcq_book_option* opts, int n, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc,
                    int mode, mcq_book_result* out, mcq_book_stats* stats);
 
+/* The same book built up incrementally (the submit / run form of the batched path).  A book
+ * object copies every option it is given (arrays included), so the caller's arrays may be freed
+ * after mcq_book_submit returns.  mcq_book_run prices everything submitted so far, in
+ * submission order, exactly as mcq_book_price; mcq_book_clear empties the book.  Not
+ * re-entrant per book object. */
+typedef struct mcq_book_s* mcq_book;
+int mcq_book_create(mcq_book* out);
+int mcq_book_submit(mcq_book b, const mcq_book_option* opts, int n);   /* appends n options */
+int mcq_book_size(mcq_book b, int* n);
+int mcq_book_run(mcq_book b, const mcq_mlmc_cfg* ml, const mcq_qmc_cfg* qc, int mode,
+                 mcq_book_result* out, mcq_book_stats* stats);         /* out: one per option */
+int mcq_book_clear(mcq_book b);
+int mcq_book_free(mcq_book b);
+
 /* ---------------------------------------------------------------- hot-path passes
  * One fused kernel pass over R replicas x n_points scrambled-Sobol points (salts
  * salt_base + r, point indices offset .. offset + n_points - 1).  sums_host receives

@@ -124,3 +124,28 @@ def test_oracle_basket_level0_matches_the_uncoupled_path(eng, orc):
     yf, yc, _ = orc.basket_level(m, p, 16, 0, z)
     assert yc == 0.0
     assert abs(yf - orc.path_payoff(m, p, 16, z)) < 1e-12 * (1 + abs(yf))
+
+
+def test_book_object_copies_and_validates(eng):
+    """mcq_book_create / submit / size / clear / free without a GPU: the book copies its options
+    (the caller's arrays may go away) and rejects bad ones at submission."""
+    b = eng.Book()
+    assert len(b) == 0
+    opts = [_one(eng, d=d) for d in (1, 5, 16)]
+    b.submit(opts)
+    del opts
+    import gc
+    gc.collect()
+    assert len(b) == 3
+    b.submit([_one(eng, d=2)])
+    assert len(b) == 4
+    with pytest.raises(eng.MCQError) as e:
+        b.submit([_one(eng, d=17)])
+    assert e.value.code == 3 and len(b) == 4          # nothing appended on error
+    b.clear()
+    assert len(b) == 0
+    L = eng.lib()
+    ml, qc = eng.mlmc_cfg(M=2, n0_steps=1), eng.qmc_cfg(R=16)
+    out = (eng.mcq_types.BookResult * 1)()
+    assert L.mcq_book_run(b.h, C.byref(ml), C.byref(qc), 0, out, None) == 1   # empty book
+    b.close()

@@ -224,3 +224,19 @@ def test_book_state_machine_matches_python_restatement(gpu):
         assert (b["levels"], b["n_samples"], b["converged"]) == (ref["levels"], ref["n_samples"], ref["converged"])
         assert b["price"] == ref["price"] and b["std_error"] == ref["std_error"], (b, ref)
         assert np.array_equal(b["delta"], ref["delta"])
+
+
+def test_book_object_run_equals_book_price(gpu):
+    """The submit / run book object prices exactly as mcq_book_price on the same options."""
+    opts = gpu.config5_book(n=10, seed=33)
+    for o in opts:
+        o.eps = 10 * o.eps
+    ref, _ = gpu.book_price(opts, gpu.BOOK_BATCHED)
+    b = gpu.Book()
+    b.submit(opts[:4])
+    b.submit(opts[4:])
+    out, st = b.run(gpu.BOOK_BATCHED)
+    b.close()
+    for r, o, x in zip(ref, opts, out):
+        assert r["price"] == x.price and r["std_error"] == x.std_error and r["n_samples"] == x.n_samples
+        assert np.array_equal(r["delta"], np.array(x.delta[:o.n_assets]))
