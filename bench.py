@@ -131,6 +131,39 @@ def cpu_baseline(seconds=12.0, steps=1):
             "sample": f"{REPS} replicas x {n} points x {STEPS} steps of the same workload (FP64 oracle)"}
 
 
+def configs_bench(eng):
+    """The other workloads of the benchmark suite through the public API, host wall time of one
+    warm call each: plain MC (GBM European, 64 Euler steps, Philox, pilot 2^14, eps 1e-2),
+    MLQMC for Heston (kappa 2, theta 0.04, xi 0.3, rho -0.7, v0 0.04, S0 100, r 0.02, T 1; M 4,
+    4 steps on level 0, L <= 8, R 16, eps 1e-3) with a lookback and a down-and-out call
+    (K 100, B 80), and the pathwise adjoint on the 64 x 32 local-vol grid (Asian call, T 2,
+    512 steps, 16 x 2^18 scrambled paths, price + delta + rho + 2048 node vegas)."""
+    out = {}
+
+    def timed(fn):
+        fn()
+        t0 = time.perf_counter()
+        r = fn()
+        return r, time.perf_counter() - t0
+
+    m, p = eng.gbm(100.0, 0.05, 0.2, 1.0), eng.european(100.0, 0.05, 1.0)
+    r, t = timed(lambda: eng.run_mc(m, p, 1e-2, 64, eng.mc_cfg(pilot_n=1 << 14)))
+    out["mc_gbm_european"] = {"price": r["price"], "std_error": r["std_error"], "time_s": t,
+                              "path_steps_per_s": r["path_steps"] / t}
+    h = eng.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)
+    for name, pay in (("lookback", eng.lookback(0.2)), ("down_out", eng.barrier_down_out(100.0, 80.0, 0.2, 0.02, 1.0))):
+        r, t = timed(lambda: eng.run_mlqmc(h, pay, 1e-3, eng.mlmc_cfg(M=4, n0_steps=4, max_L=8), eng.qmc_cfg(R=16)))
+        out["mlqmc_heston_" + name] = {"price": r["price"], "std_error": r["std_error"], "levels": r["levels"],
+                                       "time_s": t, "path_steps_per_s": r["path_steps"] / t}
+    K, tt, grid = eng.config4_surface()
+    lv = eng.localvol_grid(K, tt, grid, 100.0, 0.05, 2.0)
+    (g, _), t = timed(lambda: eng.adjoint(lv, eng.asian(100.0), 512, salt_base=42, R=16, n_points=1 << 18))
+    out["adjoint_localvol_asian"] = {"price": g["price"], "delta": g["delta"], "rho": g["rho"], "vega": g["vega"],
+                                     "time_s": t, "path_steps_per_s": g["path_steps"] / t,
+                                     "paths_per_s": g["n_paths"] / t}
+    return out
+
+
 def book_bench(eng, n):
     """The batched heterogeneous book against its plain form on the same GPU: the first n options
     of the 4096-option synthetic book (d ~ U{1..16}, correlated GBM, Dirichlet weights, T ~
@@ -247,6 +280,7 @@ def main():
     ap.add_argument("--no-variants", action="store_true", help="skip the bridge / PCA orderings")
     ap.add_argument("--book-options", type=int, default=64,
                     help="options of the synthetic basket book priced batched and plain (0: skip)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the MC / Heston MLQMC / adjoint workloads")
     ap.add_argument("--book-slice", default=None, metavar="D:LEVEL[:POINTS]",
                     help="only price one slice of a D-asset basket at LEVEL through the book kernel "
                          "(R = 16, M = 2, n0 = 1) and print its normals/s: the profiling case")
@@ -356,6 +390,7 @@ def main():
     h2d_e2e = ctypes.sizeof(m) + ctypes.sizeof(p) + ctypes.sizeof(cfg)
 
     book = None if args.book_options <= 0 else book_bench(eng, args.book_options)
+    others = None if args.no_configs else configs_bench(eng)
 
     if world > 1:
         import torch.distributed as dist
@@ -406,6 +441,8 @@ def main():
     }
     if book is not None:
         line["book"] = book
+    if others is not None:
+        line["other_workloads"] = others
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
