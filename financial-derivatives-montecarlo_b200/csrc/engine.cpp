@@ -216,6 +216,11 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
         k.em_c = (float)std::exp((double)(-k.kappa * k.hc));
         if (a.level0) k.M = INT_MAX;   // the coarse path never steps on level 0
     }
+    if (m.kind == MCQ_MODEL_HESTON && (a.flags & MCQ_FLAG_HESTON_MILSTEIN)) {
+        k.mil = 0.25f * k.xi * k.xi;
+        k.mil_hf = k.mil * k.h;
+        k.mil_hc = k.mil * (k.hc > 0.f ? k.hc : k.h);
+    }
 
     k.K = (float)p.K;
     k.B = (float)p.B;

@@ -48,6 +48,7 @@ struct KParams {
     float kappa, theta, xi, L10, L11, v0, em_f;    // em_f = exp(-kappa h)
     float sigma0, alpha, bm1;                      // Dupire: bm1 = beta_d - 1
     float hc, em_c;                                // coarse step, exp(-kappa hc)
+    float mil, mil_hf, mil_hc;                     // Heston Milstein: xi^2/4 and its h, hc multiples (0: Euler)
     // ---- payoff
     float K, B, disc, corr_f, corr_c, u_cap;
     float pay_T;                                   // payoff maturity (discount sensitivity)

@@ -271,7 +271,7 @@ struct Leg {
     }
     template <bool RUN>
     __device__ __forceinline__ void step(const KParams& p, float dw1, float dw2, float t,
-                                         float muh, float em) {
+                                         float muh, float em, float milh) {
         if constexpr (MOD == MOD_GBM) {
             S = fmaf(S, fmaf(p.sigma, dw1, muh), S);
         } else if constexpr (MOD == MOD_DUPIRE) {
@@ -284,6 +284,7 @@ struct Leg {
             const float sq = sqrtf(fmaxf(V, 0.f));
             S = fmaf(S, fmaf(sq, dw1, muh), S);
             V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
+            if (p.mil != 0.f) V = fmaf(p.mil, dw2 * dw2, V - milh);   // Milstein: xi^2/4 (dW^2 - h)
         }
         if constexpr (RUN && path_dep<PAY>()) update();
     }
@@ -325,16 +326,16 @@ struct PathC {
     }
     __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
         const float t = (float)k * p.h;
-        if (run_upd) f.template step<true>(p, dw1, dw2, t, muh_f, p.em_f);
-        else f.template step<false>(p, dw1, dw2, t, muh_f, p.em_f);
+        if (run_upd) f.template step<true>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
+        else f.template step<false>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
         k++;
         if constexpr (COUPLED) {
             a1 += dw1;
             if constexpr (HES) a2 += dw2;
             if (++m == p.M) {
                 const float tc = (float)ck * p.hc;
-                if (run_upd) c.template step<true>(p, a1, a2, tc, muh_c, p.em_c);
-                else c.template step<false>(p, a1, a2, tc, muh_c, p.em_c);
+                if (run_upd) c.template step<true>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
+                else c.template step<false>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
                 a1 = a2 = 0.f; m = 0; ck++;
             }
         }

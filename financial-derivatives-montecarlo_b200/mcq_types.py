@@ -13,6 +13,7 @@ EUROPEAN, ASIAN, GEOM_ASIAN, LOOKBACK, BARRIER_UP_OUT, BASKET, BARRIER_DOWN_OUT 
 RAW, BB, PCA = range(3)
 FLAG_COMPAT_U_INF = 1
 FLAG_COMPAT_HESTON_MLMC = 2
+FLAG_HESTON_MILSTEIN = 8
 
 _pd = C.POINTER(C.c_double)
 

@@ -66,6 +66,9 @@ extern "C" {
                                            default maps that single float to 1 - 2^-24 */
 #define MCQ_FLAG_COMPAT_HESTON_MLMC  2  /* skip the running (path-dependent) update on the
                                            Heston coupled path, as methods_cuda.cu:464-490 */
+#define MCQ_FLAG_HESTON_MILSTEIN     8  /* Heston variance step with the Milstein term
+                                           xi^2/4 (dW2^2 - h) (Euler-Milstein, full truncation);
+                                           default: the reference's Euler step (:276-284) */
 
 /* ---------------------------------------------------------------- parameter structs */
 typedef struct mcq_model {

@@ -484,6 +484,13 @@ static void make_increments(const mcq_model* m, int n_steps, const orc_noise* nz
 /* kernel_mc / d_step / kernel_multi_dupire (methods_cuda.cu:388-437, 525-551) in FP64. */
 double orc_path_payoff(const mcq_model* m, const mcq_payoff* p, int n_steps,
                        const orc_noise* nz, const double* z) {
+    return orc_path_payoff_f(m, p, n_steps, nz, z, 0);
+}
+
+/* as orc_path_payoff; flags & MCQ_FLAG_HESTON_MILSTEIN adds the Milstein term
+   xi^2/4 (dW2^2 - h) to the Heston variance step */
+double orc_path_payoff_f(const mcq_model* m, const mcq_payoff* p, int n_steps,
+                         const orc_noise* nz, const double* z, int flags) {
     int d = orc_noise_dim(m), D = n_steps * d;
     double h = m->T / n_steps;
     double* dW = (double*)malloc(sizeof(double) * D);
@@ -536,6 +543,7 @@ double orc_path_payoff(const mcq_model* m, const mcq_payoff* p, int n_steps,
                     double Vp = V > 0 ? V : 0, sq = sqrt(Vp);
                     S = S + m->mu * S * h + sq * S * dw1;
                     V = m->theta + em * (V - m->theta) + m->xi * sq * dw2;
+                    if (flags & MCQ_FLAG_HESTON_MILSTEIN) V += 0.25 * m->xi * m->xi * (dw2 * dw2 - h);
                 } break;
             }
             if (path_dep(p)) run_update(p, &run, S);
@@ -572,6 +580,7 @@ double orc_level_payoff(const mcq_model* m, const mcq_payoff* p, int n_fine, int
             double Vp = Vf > 0 ? Vf : 0, sq = sqrt(Vp);
             Sf = Sf + m->mu * Sf * hf + sq * Sf * dw1;
             Vf = m->theta + emf * (Vf - m->theta) + m->xi * sq * dw2;
+            if (flags & MCQ_FLAG_HESTON_MILSTEIN) Vf += 0.25 * m->xi * m->xi * (dw2 * dw2 - hf);
         } else {
             double dw = dW[k];
             a1 += dw;
@@ -590,6 +599,7 @@ double orc_level_payoff(const mcq_model* m, const mcq_payoff* p, int n_fine, int
                 double Vp = Vc > 0 ? Vc : 0, sq = sqrt(Vp);
                 Sc = Sc + m->mu * Sc * hc + sq * Sc * a1;
                 Vc = m->theta + emc * (Vc - m->theta) + m->xi * sq * a2;
+                if (flags & MCQ_FLAG_HESTON_MILSTEIN) Vc += 0.25 * m->xi * m->xi * (a2 * a2 - hc);
             } else if (m->kind == MCQ_MODEL_GBM) {
                 Sc = Sc + m->mu * Sc * hc + m->sigma * Sc * a1;
             } else if (m->kind == MCQ_MODEL_DUPIRE) {
@@ -657,7 +667,7 @@ int orc_qmc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, const orc
                 for (int dd = 0; dd < D; dd++) x[dd] ^= L[dd * 33 + k];
             }
             for (int dd = 0; dd < D; dd++) z[dd] = orc_ppnd16((double)orc_u_of(x[dd], flags));
-            double y = orc_path_payoff(m, p, n_steps, nz, z);
+            double y = orc_path_payoff_f(m, p, n_steps, nz, z, flags);
             s1 += y; s2 += y * y;
         }
         part[task * 2] = s1; part[task * 2 + 1] = s2;

@@ -75,6 +75,8 @@ typedef struct orc_noise {
 int    orc_noise_dim(const mcq_model* m);
 double orc_path_payoff(const mcq_model* m, const mcq_payoff* p, int n_steps,
                        const orc_noise* nz, const double* z);
+double orc_path_payoff_f(const mcq_model* m, const mcq_payoff* p, int n_steps,
+                         const orc_noise* nz, const double* z, int flags);
 /* coupled fine/coarse pair (kernel_mlmc, methods_cuda.cu:445-518): returns Yf, *yc = Yc */
 double orc_level_payoff(const mcq_model* m, const mcq_payoff* p, int n_fine, int M,
                         const orc_noise* nz, const double* z, int flags, double* yc);

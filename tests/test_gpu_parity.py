@@ -176,3 +176,22 @@ def test_bridge_launch_variants_are_bit_identical(gpu, model, pay):
         os.environ.pop("MCQ_TUNE", None)
         bb.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("pay", ["eur", "lookback", "downout"])
+def test_heston_milstein_flag(gpu, orc, pay):
+    """MCQ_FLAG_HESTON_MILSTEIN (Euler-Milstein variance step): single-level and coupled level
+    sums against the FP64 oracle with the same flag, and the flag changes the result."""
+    m, p = make_model(gpu, "heston"), make_payoff(gpu, pay)
+    F, N, R = gpu.FLAG_HESTON_MILSTEIN, 1024, 2
+    g = gpu.qmc_pass(m, p, 64, salt_base=42, R=R, offset=0, n_points=N, flags=F)
+    o = orc.qmc_sums(m, p, 64, None, salt_base=42, R=R, offset=0, N=N, flags=F)
+    e = orc.qmc_sums(m, p, 64, None, salt_base=42, R=R, offset=0, N=N, flags=0)
+    for r in range(R):
+        assert abs(g[r, 0] / N - o[r, 0] / N) < tol(pay, N, o[r, 0] / N), (r, g[r], o[r])
+    assert np.abs(o[:, 1] - e[:, 1]).max() > 1e-9 * np.abs(e[:, 1]).max()   # the term is there
+    gl = gpu.level_pass(m, p, 64, 4, use_sobol=True, salt_base=7, R=R, n_points=N, flags=F)
+    ol = orc.level_sums(m, p, 64, 4, None, use_sobol=True, salt_base=7, R=R, N=N, flags=F)
+    for r in range(R):
+        for k in (0, 2):
+            assert abs(gl[r, k] / N - ol[r, k] / N) < tol(pay, N, ol[r, k] / N) * 2, (r, k, gl[r], ol[r])
