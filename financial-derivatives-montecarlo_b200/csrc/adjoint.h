@@ -5,6 +5,6 @@
 namespace mcq {
 
 const void* lookup_adjoint(int model, int payoff);
-size_t adjoint_smem_bytes(int n_steps, int n_nodes);
+size_t adjoint_smem_bytes(int model, int n_steps, int n_nodes);
 
 }  // namespace mcq

@@ -539,12 +539,17 @@ namespace mcq {
 void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t salt_base, int R,
                  uint64_t offset, uint64_t n_points, int flags, mcq_greeks& out, double* node_vega) {
     Engine& E = engine();
-    MCQ_REQUIRE(m.kind == MCQ_MODEL_GBM || m.kind == MCQ_MODEL_DUPIRE || m.kind == MCQ_MODEL_LOCALVOL_GRID,
-                MCQ_ERR_UNSUPPORTED, "adjoint Greeks: GBM, parametric Dupire or grid local-vol models");
+    MCQ_REQUIRE(m.kind == MCQ_MODEL_GBM || m.kind == MCQ_MODEL_DUPIRE || m.kind == MCQ_MODEL_LOCALVOL_GRID ||
+                    m.kind == MCQ_MODEL_HESTON,
+                MCQ_ERR_UNSUPPORTED, "adjoint Greeks: GBM, Heston, parametric Dupire or grid local-vol models");
     MCQ_REQUIRE(p.kind == MCQ_PAYOFF_EUROPEAN || p.kind == MCQ_PAYOFF_ASIAN || p.kind == MCQ_PAYOFF_LOOKBACK,
                 MCQ_ERR_UNSUPPORTED, "adjoint Greeks: European, Asian or lookback payoffs (Lipschitz)");
-    MCQ_REQUIRE(n_steps >= 32 && n_steps % 32 == 0 && n_steps <= 1024, MCQ_ERR_UNSUPPORTED,
-                "adjoint Greeks: n_steps must be a multiple of 32 in [32, 1024]");
+    if (m.kind == MCQ_MODEL_HESTON)
+        MCQ_REQUIRE(n_steps >= 16 && n_steps % 16 == 0 && n_steps <= 1024, MCQ_ERR_UNSUPPORTED,
+                    "adjoint Greeks (Heston): n_steps must be a multiple of 16 in [16, 1024]");
+    else
+        MCQ_REQUIRE(n_steps >= 32 && n_steps % 32 == 0 && n_steps <= 1024, MCQ_ERR_UNSUPPORTED,
+                    "adjoint Greeks: n_steps must be a multiple of 32 in [32, 1024]");
     MCQ_REQUIRE(R >= 1 && n_points >= 1 && offset + n_points <= (1ull << 32), MCQ_ERR_RANGE, "bad replica / point range");
     auto t0 = std::chrono::steady_clock::now();
     const int l0 = E.launches;
@@ -566,11 +571,11 @@ void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t 
     const uint64_t ipr = (G + gpi - 1) / gpi;
     k.R = R; k.gpi = (int)gpi; k.items_per_rep = (int)ipr; k.n_items = (int)(ipr * R);
     k.offset = offset; k.n_points = n_points; k.g0 = g0; k.G = G;
-    if (!(ws.dirs_salt0 == salt_base && ws.dirs_R == R && ws.dirs_D == n_steps)) {
-        uint32_t* d = (uint32_t*)ws.dirs.ensure(sizeof(uint32_t) * (size_t)R * 33 * n_steps);
-        launch_prescramble(E.d_dv, salt_base, R, n_steps, d, ws.stream);
+    if (!(ws.dirs_salt0 == salt_base && ws.dirs_R == R && ws.dirs_D == k.D)) {
+        uint32_t* d = (uint32_t*)ws.dirs.ensure(sizeof(uint32_t) * (size_t)R * 33 * k.D);
+        launch_prescramble(E.d_dv, salt_base, R, k.D, d, ws.stream);
         E.launches++;
-        ws.dirs_salt0 = salt_base; ws.dirs_R = R; ws.dirs_D = n_steps;
+        ws.dirs_salt0 = salt_base; ws.dirs_R = R; ws.dirs_D = k.D;
     }
     k.dirs = (const uint32_t*)ws.dirs.p;
     k.nstat = 4;
@@ -581,7 +586,7 @@ void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t 
         MCQ_CUDA(cudaMemsetAsync(d_nodes, 0, sizeof(double) * n_nodes, ws.stream));
     }
     k.node_out = d_nodes;
-    const size_t smem = adjoint_smem_bytes(n_steps, n_nodes);
+    const size_t smem = adjoint_smem_bytes(k.model, n_steps, n_nodes);
     KernelInfo& ki = kernel_info(fn, smem);
     long long blocks = std::min<long long>(((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock,
                                            (long long)ki.blocks_per_sm * E.sm_count);

@@ -13,7 +13,7 @@
 // European (discounted), arithmetic Asian and floating-strike lookback (BGK factor constant).
 // Per path it yields P, delta = Sbar_0, rho = mubar (+ -T P for the discounted European, the
 // drift and the discount sharing the rate) and vega (GBM: d/dsigma; Dupire: d/dsigma0; grid:
-// the parallel shift = sum of node vegas).
+// the parallel shift = sum of node vegas; Heston: d/dv0, see k_adjoint_heston).
 #include "adjoint.h"
 #include "path_kernels.cuh"
 
@@ -203,6 +203,128 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
     }
 }
 
+// Heston (two normals per step: dims 2k for the price, 2k + 1 for the variance, correlated by the
+// Cholesky row (L10, L11)), the pricing pass's Euler step with full truncation in the square
+// root (and, with MCQ_FLAG_HESTON_MILSTEIN, the Milstein term, which does not depend on V):
+//     S' = S + S (mu h + sqrt(V+) dW1),   V' = theta + e^{-kappa h} (V - theta) + xi sqrt(V+) dW2.
+// The reverse sweep carries (Sbar, Vbar):
+//     Sbar_k = Sbar_{k+1} (1 + mu h + sqrt(V+) dW1) + dP/dS_k,
+//     Vbar_k = Sbar_{k+1} S_k dW1 s'(V_k) + Vbar_{k+1} (e^{-kappa h} + xi dW2 s'(V_k)),
+// with s'(V) = 1 / (2 sqrt V) for V > 0 and the subgradient 0 where the truncation is active.
+// Outputs per path: P, delta = Sbar_0, rho = mubar (- T P for the discounted European) and
+// vega = Vbar_0 = dP/dv0.  A 32-dimension Sobol tile is 16 steps, which is also the checkpoint
+// interval: (S, V) are kept at every tile boundary.
+__device__ __forceinline__ void heston_adj_step(const KParams& p, float& S, float& V, float dw1, float dw2,
+                                                float muh) {
+    const float sq = sqrtf(fmaxf(V, 0.f));
+    S = fmaf(S, fmaf(sq, dw1, muh), S);
+    V = fmaf(p.xi * sq, dw2, fmaf(p.em_f, V - p.theta, p.theta));
+    if (p.mil != 0.f) V = fmaf(p.mil, dw2 * dw2, V - p.mil_hf);
+}
+
+template <int PAY>
+__global__ void __launch_bounds__(kThreads, 1) k_adjoint_heston(const __grid_constant__ KParams p) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int N = p.n_steps, D = 2 * N, n_tiles = D / 32;
+    const int per_warp = 1024 + (n_tiles + 1) * 64 + 16 * 64;
+    float* wbase = reinterpret_cast<float*>(smem4) + wib * per_warp;
+    float* buf = wbase;                       // 32 x 32 transpose tile
+    float* ckS = wbase + 1024;                // (S, V) at every tile boundary [n_tiles + 1][32]
+    float* ckV = ckS + (n_tiles + 1) * 32;
+    float* segS = ckV + (n_tiles + 1) * 32;   // the recomputed tile [16][32]
+    float* segV = segS + 16 * 32;
+    const float h = p.h, sqh = p.sqrt_h, muh = p.mu * p.h;
+    const int total_warps = gridDim.x * kWarpsPerBlock;
+    const uint64_t gend_all = p.g0 + p.G;
+    for (int item = blockIdx.x * kWarpsPerBlock + wib; item < p.n_items; item += total_warps) {
+        const int r = item / p.items_per_rep;
+        const int j = item - r * p.items_per_rep;
+        const uint64_t gb = p.g0 + (uint64_t)j * (uint64_t)p.gpi;
+        const uint64_t ge = min(gb + (uint64_t)p.gpi, gend_all);
+        const uint32_t* dr = p.dirs + (size_t)r * 33 * (size_t)D;
+        Acc<4> acc;
+        acc.zero();
+        for (uint64_t hg = gb; hg < ge; hg++) {
+            const uint64_t n = hg * 32 + (uint64_t)lane;
+            const bool valid = n >= p.offset && n < p.offset + p.n_points;
+            // ---------------- forward sweep
+            float S = p.S0, V = p.v0, ts = 0.f, tot = 0.f, comp = 0.f, mn = p.S0;
+            int kmin = 0;
+            for (int t = 0; t < n_tiles; t++) {
+                ckS[t * 32 + lane] = S;
+                ckV[t * 32 + lane] = V;
+                sobol_tile(dr, D, t * 32 + lane, true, hg, p.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const float z1 = z[2 * i], z2 = z[2 * i + 1];
+                    heston_adj_step(p, S, V, z1 * sqh, fmaf(p.L10, z1, p.L11 * z2) * sqh, muh);
+                    if constexpr (PAY == PAY_ASIAN) ts += S;
+                    if constexpr (PAY == PAY_LOOKBACK) {
+                        if (S < mn) { mn = S; kmin = t * 16 + i + 1; }
+                    }
+                }
+                if constexpr (PAY == PAY_ASIAN) { kadd(tot, comp, ts); ts = 0.f; }
+            }
+            float P, g_all = 0.f, Sbar;
+            if constexpr (PAY == PAY_EUR) {
+                P = fmaxf(S - p.K, 0.f) * p.disc;
+                Sbar = (S > p.K) ? p.disc : 0.f;
+            } else if constexpr (PAY == PAY_ASIAN) {
+                const float A = (tot - comp) / (float)N;
+                P = fmaxf(A - p.K, 0.f);
+                g_all = (A > p.K) ? 1.f / (float)N : 0.f;
+                Sbar = g_all;
+            } else {   // floating-strike lookback
+                P = S - mn * p.corr_f;
+                Sbar = 1.f + ((kmin == N) ? -p.corr_f : 0.f);
+            }
+            // ---------------- reverse sweep
+            float mubar = 0.f, Vbar = 0.f;
+            for (int t = n_tiles - 1; t >= 0; t--) {
+                sobol_tile(dr, D, t * 32 + lane, true, hg, p.u_cap, buf, lane);
+                __syncwarp();
+                float z[32];
+                read_row(buf, lane, z);
+                __syncwarp();
+                float Sr = ckS[t * 32 + lane], Vr = ckV[t * 32 + lane];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    segS[i * 32 + lane] = Sr;
+                    segV[i * 32 + lane] = Vr;
+                    const float z1 = z[2 * i], z2 = z[2 * i + 1];
+                    heston_adj_step(p, Sr, Vr, z1 * sqh, fmaf(p.L10, z1, p.L11 * z2) * sqh, muh);
+                }
+#pragma unroll
+                for (int i = 15; i >= 0; i--) {
+                    const int k = t * 16 + i;
+                    const float Sk = segS[i * 32 + lane], Vk = segV[i * 32 + lane];
+                    const float z1 = z[2 * i], z2 = z[2 * i + 1];
+                    const float dw1 = z1 * sqh, dw2 = fmaf(p.L10, z1, p.L11 * z2) * sqh;
+                    const float sq = sqrtf(fmaxf(Vk, 0.f));
+                    const float dsq = (Vk > 0.f) ? 0.5f / sq : 0.f;
+                    mubar = fmaf(Sbar, Sk * h, mubar);
+                    const float nV = fmaf(Sbar, Sk * dw1 * dsq, Vbar * fmaf(p.xi * dw2, dsq, p.em_f));
+                    float direct = 0.f;
+                    if constexpr (PAY == PAY_ASIAN) direct = (k >= 1) ? g_all : 0.f;
+                    if constexpr (PAY == PAY_LOOKBACK) direct = (k == kmin) ? -p.corr_f : 0.f;
+                    Sbar = fmaf(Sbar, 1.f + muh + sq * dw1, direct);
+                    Vbar = nV;
+                }
+            }
+            float rho = mubar;
+            if constexpr (PAY == PAY_EUR) rho -= p.pay_T * P;
+            float y[4] = {P, Sbar, rho, Vbar};
+            if (valid) acc.add(y);
+        }
+        acc.flush(p.partials + (size_t)item * 4, lane);
+    }
+}
+
 template <int MOD>
 static const void* adj_payoff(int pay) {
     switch (pay) {
@@ -218,11 +340,22 @@ const void* lookup_adjoint(int model, int payoff) {
         case MOD_GBM: return adj_payoff<MOD_GBM>(payoff);
         case MOD_DUPIRE: return adj_payoff<MOD_DUPIRE>(payoff);
         case MOD_LVGRID: return adj_payoff<MOD_LVGRID>(payoff);
+        case MOD_HESTON:
+            switch (payoff) {
+                case PAY_EUR: return (const void*)&k_adjoint_heston<PAY_EUR>;
+                case PAY_ASIAN: return (const void*)&k_adjoint_heston<PAY_ASIAN>;
+                case PAY_LOOKBACK: return (const void*)&k_adjoint_heston<PAY_LOOKBACK>;
+                default: return nullptr;
+            }
         default: return nullptr;
     }
 }
 
-size_t adjoint_smem_bytes(int n_steps, int n_nodes) {
+size_t adjoint_smem_bytes(int model, int n_steps, int n_nodes) {
+    if (model == MOD_HESTON) {
+        const int n_tiles = 2 * n_steps / 32;
+        return (size_t)kWarpsPerBlock * (1024 + (n_tiles + 1) * 64 + 16 * 64) * sizeof(float);
+    }
     const int n_ck = n_steps / kCk + 1;
     const size_t per_warp = (size_t)(1024 + n_ck * 32 + kCk * 32) * sizeof(float);
     return (size_t)((n_nodes + 1) & ~1) * sizeof(double) + kWarpsPerBlock * per_warp;

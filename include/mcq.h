@@ -250,11 +250,12 @@ int mcq_run_is(const mcq_model* gbm, const mcq_payoff* european, double z_star, 
  * Pathwise adjoint Greeks over R scrambled-Sobol replicas (salts salt_base + r, points offset ..
  * offset + n_points - 1); no counterpart in the reference, which computes no Greeks.
  * delta = dV/dS0, rho = dV/d(rate) with the drift mu and the payoff's discount rate moving
- * together, vega = dV/dsigma (GBM), dV/dsigma0 (parametric Dupire) or the parallel shift of the
- * local-vol grid; node_vega (optional, lv_nt * lv_nK doubles, same layout as lv_sigma) receives
- * dV/dsigma(K_i, t_j).  Lipschitz payoffs only: European, arithmetic Asian, lookback.
- * n_steps: multiple of 32 in [32, 1024]; path states are checkpointed every 16 steps and
- * recomputed in the reverse sweep. */
+ * together, vega = dV/dsigma (GBM), dV/dsigma0 (parametric Dupire), the parallel shift of the
+ * local-vol grid, or dV/dv0 (Heston; full-truncation subgradient where V <= 0, and the Milstein
+ * step with MCQ_FLAG_HESTON_MILSTEIN); node_vega (optional, lv_nt * lv_nK doubles, same layout
+ * as lv_sigma) receives dV/dsigma(K_i, t_j).  Lipschitz payoffs only: European, arithmetic Asian,
+ * lookback.  n_steps: multiple of 32 in [32, 1024] (Heston: of 16 in [16, 1024]); path states
+ * are checkpointed every 16 steps and recomputed in the reverse sweep. */
 int mcq_adjoint(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t salt_base, int R,
                 uint32_t offset, int64_t n_points, int flags, mcq_greeks* out, double* node_vega);
 

@@ -130,3 +130,42 @@ def test_torch_autograd_wrapper(gpu):
     m = lambda s0, sg, u: McqPrice.apply(torch.tensor(s0), torch.tensor(sg), torch.tensor(u)).item()
     assert abs(dS.item() - (m(100 + h, 0.25, 0.03) - m(100 - h, 0.25, 0.03)) / (2 * h)) < 1e-3
     assert abs(dsig.item() - (m(100, 0.25 + 1e-4, 0.03) - m(100, 0.25 - 1e-4, 0.03)) / 2e-4) < 2e-2
+
+
+def _heston_price(orc, m, p, n, salt, N, flags):
+    s = orc.qmc_sums(m, p, n, None, salt, 1, 0, N, flags)
+    return s[0, 0] / N
+
+
+@pytest.mark.parametrize("pay,flags", [("eur", 0), ("asian", 0), ("lookback", 0), ("asian", 8)])
+def test_heston_adjoint_vs_fp64_finite_differences(gpu, orc, pay, flags):
+    """Heston (full truncation; flags 8 adds the Milstein variance term): pathwise delta, rho and
+    dP/dv0 against FP64 central differences of the oracle on the same scrambled points."""
+    T = orc.T
+    S0, mu, kap, th, xi, rho_c, v0 = 100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04
+    n, N = 64, 4096
+
+    def model(S0=S0, mu=mu, v0=v0):
+        return T.heston(S0, mu, kap, th, xi, rho_c, v0, 1.0)
+
+    p = {"eur": T.european(100.0, mu, 1.0), "asian": T.asian(100.0), "lookback": T.lookback(0.2)}[pay]
+    g, _ = gpu.adjoint(model(), p, n, salt_base=7, R=1, n_points=N, flags=flags)
+
+    def fd(build, x0, rel=1e-4):
+        hh = rel * x0
+        return (_heston_price(orc, build(x0 + hh), p, n, 7, N, flags) -
+                _heston_price(orc, build(x0 - hh), p, n, 7, N, flags)) / (2 * hh)
+
+    delta = fd(lambda x: model(S0=x), S0)
+    vega = fd(lambda x: model(v0=x), v0)
+    if pay == "eur":   # the drift and the discount share the rate
+        rho = fd(lambda x: model(mu=x), mu)
+        pu, pd = T.european(100.0, mu + 1e-6, 1.0), T.european(100.0, mu - 1e-6, 1.0)
+        rho += (orc.qmc_sums(model(), pu, n, None, 7, 1, 0, N, flags)[0, 0] -
+                orc.qmc_sums(model(), pd, n, None, 7, 1, 0, N, flags)[0, 0]) / N / 2e-6
+    else:
+        rho = fd(lambda x: model(mu=x), mu)
+    price = _heston_price(orc, model(), p, n, 7, N, flags)
+    assert abs(g["price"] - price) < 2e-4 * max(1.0, abs(price)), (g["price"], price)
+    for name, ref in (("delta", delta), ("rho", rho), ("vega", vega)):
+        assert abs(g[name] - ref) < 2e-3 * max(1.0, abs(ref)), (pay, name, g[name], ref)
