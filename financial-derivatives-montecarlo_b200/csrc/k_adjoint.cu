@@ -11,7 +11,9 @@
 // and, for the grid local-vol model, adds Sbar_{k+1} S_k dW_k w_n to the four bilinear nodes n of
 // (S_k, t_k) in an FP64 shared-memory array per CTA.  Payoffs are the Lipschitz ones:
 // European (discounted), arithmetic Asian and floating-strike lookback (BGK factor constant).
-// Per path it yields P, delta = Sbar_0, rho = mubar (+ -T P for the discounted European, the
+// Per path it yields P, delta = Sbar_0 (plus, for the parametric Dupire model, whose volatility
+// (S/S0)^(beta-1) is scaled by S0, the sensitivity through that scale, so that delta is the
+// derivative of the price with respect to the model's S0), rho = mubar (+ -T P for the discounted European, the
 // drift and the discount sharing the rate) and vega (GBM: d/dsigma; Dupire: d/dsigma0; grid:
 // the parallel shift = sum of node vegas; Heston: d/dv0, see k_adjoint_heston).
 #include "adjoint.h"
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                 Sbar = 1.f + ((kmin == N) ? -p.corr_f : 0.f);
             }
             // ---------------- reverse sweep
-            float mubar = 0.f, sigbar = 0.f;
+            float mubar = 0.f, sigbar = 0.f, s0bar = 0.f;
             for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
@@ -173,6 +175,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                         mubar = fmaf(Sbar, Sk * h, mubar);
                         const float sens = Sbar * Sk * dw;     // dP/dsigma_k through this step
                         sigbar = fmaf(sens, dsP, sigbar);
+                        // the parametric Dupire volatility is scaled by the model's S0 itself:
+                        // d sigma_k / d S0 = -(beta - 1) sigma_k / S0 enters the delta
+                        if constexpr (MOD == MOD_DUPIRE) s0bar = fmaf(sens, -p.bm1 * sig * p.inv_S0, s0bar);
                         if constexpr (MOD == MOD_LVGRID) {
                             if (valid && sens != 0.f) {
                                 atomicAdd(&nodes[lv.n00], (double)(sens * lv.w00));
@@ -191,7 +196,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             }
             float rho = mubar;
             if constexpr (PAY == PAY_EUR) rho -= p.pay_T * P;
-            float y[4] = {P, Sbar, rho, sigbar};
+            float y[4] = {P, Sbar + s0bar, rho, sigbar};
             if (valid) acc.add(y);
         }
         acc.flush(p.partials + (size_t)item * 4, lane);

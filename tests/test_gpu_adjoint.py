@@ -169,3 +169,44 @@ def test_heston_adjoint_vs_fp64_finite_differences(gpu, orc, pay, flags):
     assert abs(g["price"] - price) < 2e-4 * max(1.0, abs(price)), (g["price"], price)
     for name, ref in (("delta", delta), ("rho", rho), ("vega", vega)):
         assert abs(g[name] - ref) < 2e-3 * max(1.0, abs(ref)), (pay, name, g[name], ref)
+
+
+@pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("heston", "eur"), ("heston", "asian"), ("gbm", "lookback"),
+                                       ("dupire", "asian"), ("dupire", "lookback")])
+def test_adjoint_delta_vs_bump_and_revalue_through_the_pricer(gpu, model, pay):
+    """Pathwise delta against bump-and-revalue of the pricing pass itself (the restated reference
+    pricer, FP32, common scrambled points, bump 1% of S0).  Not the grid surface: its strike kinks
+    bias any central difference at a bump the FP32 pricer can resolve (it is checked against
+    converged FP64 differences above)."""
+    if model == "gbm":
+        build = lambda s: gpu.gbm(s, 0.05, 0.2, 1.0)
+    elif model == "heston":
+        build = lambda s: gpu.heston(s, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)
+    else:
+        build = lambda s: gpu.dupire(s, 0.05, 0.2, 0.5, 0.7, 1.0)
+    p = {"asian": gpu.asian(100.0), "eur": gpu.european(100.0, 0.02, 1.0), "lookback": gpu.lookback(0.2)}[pay]
+    n, N, R = 64, 1 << 15, 4
+    g, _ = gpu.adjoint(build(100.0), p, n, salt_base=5, R=R, n_points=N)
+    up = gpu.qmc_pass(build(101.0), p, n, salt_base=5, R=R, n_points=N)[:, 0].sum() / (R * N)
+    dn = gpu.qmc_pass(build(99.0), p, n, salt_base=5, R=R, n_points=N)[:, 0].sum() / (R * N)
+    bump = (up - dn) / 2.0
+    assert abs(g["delta"] - bump) < 5e-3 * max(1.0, abs(bump)), (model, pay, g["delta"], bump)
+
+
+@pytest.mark.parametrize("pay", ["eur", "asian", "lookback"])
+def test_dupire_adjoint_vs_fp64_finite_differences(gpu, orc, pay):
+    """Parametric Dupire: delta (with respect to the model's S0, which also scales the local
+    volatility), vega = dP/dsigma0 and rho against FP64 central differences of the oracle."""
+    T = orc.T
+    mu, s0, al, be = 0.05, 0.2, 0.5, 0.7
+    n, N = 64, 4096
+    p = {"eur": T.european(100.0, mu, 1.0), "asian": T.asian(100.0), "lookback": T.lookback(0.2)}[pay]
+    g, _ = gpu.adjoint(gpu.dupire(100.0, mu, s0, al, be, 1.0), p, n, salt_base=7, R=1, n_points=N)
+    delta = fd(orc, lambda x: T.dupire(x, mu, s0, al, be, 1.0), p, n, 100.0)
+    vega = fd(orc, lambda x: T.dupire(100.0, mu, x, al, be, 1.0), p, n, s0)
+    rho = fd(orc, lambda x: T.dupire(100.0, x, s0, al, be, 1.0), p, n, mu)
+    if pay == "eur":
+        rho += (oracle_price(orc, T.dupire(100.0, mu, s0, al, be, 1.0), T.european(100.0, mu + 1e-6, 1.0), n, 7, 1, N) -
+                oracle_price(orc, T.dupire(100.0, mu, s0, al, be, 1.0), T.european(100.0, mu - 1e-6, 1.0), n, 7, 1, N)) / 2e-6
+    for name, ref in (("delta", delta), ("vega", vega), ("rho", rho)):
+        assert abs(g[name] - ref) < 5e-4 * max(1.0, abs(ref)), (pay, name, g[name], ref)
