@@ -371,7 +371,7 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
             const uint64_t key = (uint64_t)a.gen | ((uint64_t)a.noise << 4) | ((uint64_t)a.est << 8) |
                                  ((uint64_t)k.model << 12) | ((uint64_t)a.p->kind << 16);
             TuneState& ts = E.tune[key];
-            for (int v = 0; v < 2; v++) {
+            for (int v = 0; v < nvar; v++) {
                 if (ts.pending[v]) {
                     float ms = 0.f;
                     MCQ_CUDA(cudaEventSynchronize(ts.ev[v][1]));
@@ -381,13 +381,19 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
                     ts.done[v] = true;
                 }
             }
-            if (ts.chosen < 0 && ts.done[0] && ts.done[1])
-                ts.chosen = ts.per_unit[1] < ts.per_unit[0] ? 1 : 0;
+            int first_untried = -1;
+            for (int v = 0; v < nvar; v++)
+                if (!ts.done[v] && first_untried < 0) first_untried = v;
+            if (ts.chosen < 0 && first_untried < 0) {
+                ts.chosen = 0;
+                for (int v = 1; v < nvar; v++)
+                    if (ts.per_unit[v] < ts.per_unit[ts.chosen]) ts.chosen = v;
+            }
             const double units = (double)a.R * (double)a.n_points * (double)k.D;
             if (ts.chosen >= 0) {
                 variant = ts.chosen;
             } else if (units >= (double)(1 << 26)) {
-                const int v = !ts.done[0] ? 0 : 1;
+                const int v = first_untried;
                 if (!ts.pending[v]) {
                     if (!ts.ev[v][0]) {
                         MCQ_CUDA(cudaEventCreate(&ts.ev[v][0]));

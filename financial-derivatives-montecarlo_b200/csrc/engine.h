@@ -78,17 +78,18 @@ struct KernelInfo {
     size_t smem = 0;
 };
 
-// Autotuner state of one kernel family with several compiled launch variants: the first two
-// large passes run one variant each, timed by events around the kernel on its own stream; the
+// Autotuner state of one kernel family with several compiled launch variants: the first large
+// passes run one variant each, timed by events around the kernel on its own stream; the
 // variant with the lower time per path-step is kept.  Variants compute identical sums, so
 // tuning never changes a result.
+inline constexpr int kMaxVariants = 3;
 struct TuneState {
     int chosen = -1;
-    bool done[2] = {false, false};
-    bool pending[2] = {false, false};
-    double per_unit[2] = {0.0, 0.0};
-    double units[2] = {0.0, 0.0};
-    cudaEvent_t ev[2][2] = {};
+    bool done[kMaxVariants] = {};
+    bool pending[kMaxVariants] = {};
+    double per_unit[kMaxVariants] = {};
+    double units[kMaxVariants] = {};
+    cudaEvent_t ev[kMaxVariants][2] = {};
 };
 
 struct Engine {

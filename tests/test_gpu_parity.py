@@ -154,12 +154,12 @@ def test_launch_variants_are_bit_identical(gpu, model, pay):
     m, p = make_model(gpu, model), make_payoff(gpu, pay)
     out = []
     try:
-        for v in ("0", "1"):
+        for v in ("0", "1", "2"):
             os.environ["MCQ_TUNE"] = v
             out.append(gpu.qmc_pass(m, p, 64, salt_base=42, R=4, offset=3, n_points=50000))
     finally:
         os.environ.pop("MCQ_TUNE", None)
-    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
 @pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("dupire", "eur")])
