@@ -409,10 +409,11 @@ def main():
     peak_fp32 = sm_count * 128 * 2 * mhz * 1e6 / 1e12
     per_launch_ms = total_ms / args.steps
     achieved = ps_per_step * FLOPS_PER_PATH_STEP / (per_launch_ms * 1e-3) / 1e12
-    traffic = None
-    try:   # DRAM bytes of one launch from the committed ncu capture (independent of the path count)
+    traffic, issue = None, None
+    try:   # DRAM bytes of one launch and issue activity from the committed ncu capture
         with open(os.path.join(ROOT, "profiles", "traffic_k_pass.json")) as f:
-            traffic = json.load(f)["dram_bytes_per_launch"]
+            tj = json.load(f)
+        traffic, issue = tj["dram_bytes_per_launch"], tj.get("issue_active")
     except (OSError, ValueError, KeyError):
         pass
     line = {
@@ -438,7 +439,11 @@ def main():
                      "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": f"derived: {sm_count} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock "
                                     "sampled under load); MEASURED_PEAKS.json has no FP32 figure",
-                     "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel": "k_pass<Sobol, raw, PathC<GBM, Asian>>"},
+                     "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel": "k_pass<Sobol, raw, PathC<GBM, Asian>>",
+                     "issue_active_ncu": issue,
+                     "note": "instruction-issue bound: the FP32 flops are ~80% of the instructions issued, the rest "
+                             "integer (Sobol gray code, conversions) and MUFU work; issue_active_ncu is the "
+                             "fraction of cycles the schedulers issued in the committed ncu capture"},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
     }
