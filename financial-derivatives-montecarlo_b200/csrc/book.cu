@@ -75,9 +75,11 @@ struct BookArgs {
 __host__ __device__ inline int book_class(int d) { return (d - 1) >> 2; }
 
 // Per-warp shared memory: the 32 x 32 transpose tile, the option's Cholesky factor with rows
-// padded to a multiple of 4 floats, its volatilities, and the FP64 record of the chunk.
+// padded to a multiple of 4 floats, its per-asset constants (sigma, S0, weight, weight / S0), and
+// the FP64 record of the chunk.
 constexpr int kBookLsFloats = kMaxBasket * kMaxBasket;
-constexpr int kBookWarpFloats = 1024 + kBookLsFloats + kMaxBasket + 2 * kBookNST;
+constexpr int kBookAssetFloats = 4 * kMaxBasket;   // sigma, S0, weight, weight / S0 per asset
+constexpr int kBookWarpFloats = 1024 + kBookLsFloats + kBookAssetFloats + 2 * kBookNST;
 
 // The coupled basket pair of one path for a basket of exactly D assets: the correlated Euler
 // step S + S (mu h + sigma dW) with dW = L x, x = z sqrt(h), coarse steps on the summed fine
@@ -89,10 +91,11 @@ struct BookPath {
     static constexpr int DP = (D + 3) & ~3, NS = 4 + D;
     float Sf[D], Sc[D], acc[D];
     int m;
-    __device__ __forceinline__ void init(const float* bk) {
+    // as: the per-asset constants in shared memory, [sigma | S0 | weight | weight / S0]
+    __device__ __forceinline__ void init(const float* as) {
 #pragma unroll
         for (int q = 0; q < D; q++) {
-            Sf[q] = Sc[q] = __ldg(bk + q);
+            Sf[q] = Sc[q] = as[kMaxBasket + q];
             acc[q] = 0.f;
         }
         m = 0;
@@ -123,11 +126,11 @@ struct BookPath {
             m = 0;
         }
     }
-    __device__ __forceinline__ void finish(const float* bk, float K, float disc, bool has_c, float (&y)[NS]) const {
+    __device__ __forceinline__ void finish(const float* as, float K, float disc, bool has_c, float (&y)[NS]) const {
         float Bf = 0.f, Bc = 0.f;
 #pragma unroll
         for (int q = 0; q < D; q++) {
-            const float w = __ldg(bk + 2 * D + q);
+            const float w = as[2 * kMaxBasket + q];
             Bf = fmaf(w, Sf[q], Bf);
             Bc = fmaf(w, Sc[q], Bc);
         }
@@ -138,8 +141,7 @@ struct BookPath {
         y[0] = dy; y[1] = dy * dy; y[2] = yf; y[3] = yf * yf;
 #pragma unroll
         for (int q = 0; q < D; q++) {
-            const float wa = __ldg(bk + 2 * D + q) / __ldg(bk + q);
-            y[4 + q] = wa * (gf * Sf[q] - gc * Sc[q]);
+            y[4 + q] = as[3 * kMaxBasket + q] * (gf * Sf[q] - gc * Sc[q]);   // w_a / S0_a, staged per chunk
         }
     }
 };
@@ -224,8 +226,14 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
     }
     BookAcc<NS> acc;
     acc.init(wrec, lane);
-    float* sg = Ls + kBookLsFloats;   // volatilities, read from shared memory at every step
-    if (lane < D) sg[lane] = __ldg(bk + D + lane);
+    float* sg = Ls + kBookLsFloats;   // per-asset constants: sigma (read at every step), S0, w, w / S0
+    if (lane < D) {
+        const float s0 = __ldg(bk + lane), w = __ldg(bk + 2 * D + lane);
+        sg[lane] = __ldg(bk + D + lane);
+        sg[kMaxBasket + lane] = s0;
+        sg[2 * kMaxBasket + lane] = w;
+        sg[3 * kMaxBasket + lane] = w / s0;
+    }
     int nf = a.n0;
     for (int l = 0; l < s.level; l++) nf *= a.M;
     const int nc = s.level ? nf / a.M : 0;
@@ -250,7 +258,7 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
             __syncwarp();
             for (int q = 0; q < Q && g + q < ge; q++) {
                 P path;
-                path.init(bk);
+                path.init(sg);
                 for (int k = 0; k < nf; k++) {
                     float x[D];
 #pragma unroll
@@ -258,7 +266,7 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
                     path.step(x, L4, sg, muh_f, muh_c, Mc);
                 }
                 float y[NS];
-                path.finish(bk, K, disc, has_c, y);
+                path.finish(sg, K, disc, has_c, y);
                 const uint64_t n = (g + q) * 32 + (uint64_t)lane;
                 acc.add(y, n >= s.offset && n < pend, lane);
             }
@@ -267,7 +275,7 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
     } else {
         for (uint64_t g = gb; g < ge; g++) {
             P path;
-            path.init(bk);
+            path.init(sg);
             for (int k0 = 0; k0 < nf; k0 += S) {
                 const int dim = k0 * D + lane;
                 sobol_tile(dr, dstride, dim, lane < W && dim < Dt, g, a.u_cap, buf, lane);
@@ -292,7 +300,7 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
                 __syncwarp();
             }
             float y[NS];
-            path.finish(bk, K, disc, has_c, y);
+            path.finish(sg, K, disc, has_c, y);
             const uint64_t n = g * 32 + (uint64_t)lane;
             acc.add(y, n >= s.offset && n < pend, lane);
         }
@@ -308,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     float* buf = reinterpret_cast<float*>(smem4) + wib * kBookWarpFloats;
     float* Ls = buf + 1024;
-    double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats + kMaxBasket);
+    double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats + kBookAssetFloats);
     const int c_end = a.hdr[3 + CLS];
     const int s_beg = a.hdr[7 + CLS], s_last = a.hdr[8 + CLS] - 1;
     for (;;) {
