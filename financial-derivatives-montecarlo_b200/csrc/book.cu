@@ -9,11 +9,10 @@
 // replicas (salts salt_base + l R + r, shared offsets) and is cut into chunks whose size
 // depends on the slice alone.  A persistent work-queue kernel per basket-width class (d in 1-4,
 // 5-8, 9-12, 13-16, each compiled for its own register budget and specialised on the exact d)
-// pulls chunks of every option and
-// level from an atomic counter; k_book_fin turns the chunk records of each slice into {mean of
-// the replica means of dY, their sample variance, per-asset mean delta}.  The round's kernels
-// are captured once in a CUDA graph and replayed with each round's slice list (the counts are
-// read on the device).
+// pulls chunks of every option and level from an atomic counter; k_book_fin turns the chunk
+// records of each slice into {mean of the replica means of dY, their sample variance, per-asset
+// mean delta}.  The round's kernels are captured once in a CUDA graph and replayed with each
+// round's slice list (the counts are read on the device).
 //
 // The plain comparator runs the same kernels one option at a time, one launch per level on
 // that level's own stream — the reference's launch structure.  Chunk records depend only on
