@@ -189,29 +189,40 @@ def book_bench(eng, n):
         warm.append(c)
     eng.book_price(warm, eng.BOOK_BATCHED)
     eng.book_price(warm, eng.BOOK_PLAIN)
+    def both_modes(opts):
+        d, res = {}, {}
+        for name, mode in (("batched", eng.BOOK_BATCHED), ("plain", eng.BOOK_PLAIN)):
+            r, st = eng.book_price(opts, mode) if opts else ([], {"time_s": 0.0, "rounds": 0, "launches": 0,
+                                                                  "normals": 0.0, "path_steps": 0.0})
+            res[name] = r
+            agg = torch.tensor([st["time_s"], st["normals"], st["path_steps"]], dtype=torch.float64, device="cuda")
+            if world > 1:
+                t = agg[:1].clone()
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                w = agg[1:].clone()
+                torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+                agg = torch.cat([t, w])
+            tmax, normals, psteps = agg.tolist()
+            d[name] = {"options_per_s": n / tmax, "time_s": tmax, "rounds": st["rounds"],
+                       "launches": st["launches"], "normals_per_s": normals / tmax,
+                       "path_steps_per_s": psteps / tmax}
+        d["batched_over_plain"] = d["batched"]["options_per_s"] / d["plain"]["options_per_s"]
+        d["bit_identical"] = all(a["price"] == b["price"] and bool((a["delta"] == b["delta"]).all())
+                                 for a, b in zip(res["batched"], res["plain"]))
+        d["converged"] = sum(1 for x in res["batched"] if x["converged"])
+        return d
+
     out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5); "
                                      "MLQMC R=16 M=2 n0=1, per-option eps, price + per-asset delta" % n,
            "sharding": "options round-robin over %d rank(s), fixed total" % world}
-    res = {}
-    for name, mode in (("batched", eng.BOOK_BATCHED), ("plain", eng.BOOK_PLAIN)):
-        r, st = eng.book_price(mine, mode) if mine else ([], {"time_s": 0.0, "rounds": 0, "launches": 0,
-                                                               "normals": 0.0, "path_steps": 0.0})
-        res[name] = r
-        agg = torch.tensor([st["time_s"], st["normals"], st["path_steps"]], dtype=torch.float64, device="cuda")
-        if world > 1:
-            t = agg[:1].clone()
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            w = agg[1:].clone()
-            torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
-            agg = torch.cat([t, w])
-        tmax, normals, psteps = agg.tolist()
-        out[name] = {"options_per_s": n / tmax, "time_s": tmax, "rounds": st["rounds"],
-                     "launches": st["launches"], "normals_per_s": normals / tmax,
-                     "path_steps_per_s": psteps / tmax}
-    out["batched_over_plain"] = out["batched"]["options_per_s"] / out["plain"]["options_per_s"]
-    out["bit_identical"] = all(a["price"] == b["price"] and bool((a["delta"] == b["delta"]).all())
-                               for a, b in zip(res["batched"], res["plain"]))
-    out["converged"] = sum(1 for x in res["batched"] if x["converged"])
+    out.update(both_modes(mine))
+    # the same options at the metric's eps = 1e-3 each (copies; the arrays stay with `book`)
+    at = []
+    for o in mine:
+        c = type(o).from_buffer_copy(o)
+        c.eps = 1e-3
+        at.append(c)
+    out["eps_1e-3"] = both_modes(at)
     return out
 
 
