@@ -472,7 +472,8 @@ void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out)
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no tensor-core PCA kernel for this model / payoff");
     const uint64_t g0 = a.offset >> 5;
     const uint64_t G = ((a.offset + a.n_points - 1) >> 5) - g0 + 1;
-    const uint64_t tiles = (G + 7) / 8;
+    const uint64_t gpt = (uint64_t)pca_tile_paths() / 32;   // 32-point groups per tile
+    const uint64_t tiles = (G + gpt - 1) / gpt;
     const uint64_t target = 148ULL * 4;
     uint64_t tpi = (tiles * (uint64_t)a.R + target - 1) / target;
     if (tpi < 1) tpi = 1;

@@ -2,19 +2,25 @@
 //
 // The reference applies PCA as three HBM passes: cast the normals to fp16, one cuBLAS GEMM
 // dW = Z M^T over the whole [D x N] array, then the path kernel (methods_cuda.cu:1150-1166,
-// :1228-1229, :720-724).  Here one kernel does it per tile of 256 paths:
-//   1. sixteen warps generate the scrambled-Sobol normals of the tile's paths, 64 dimensions at
-//      a time (warps w and w + 8 make the two 32-dimension halves of the rows of paths 32(w mod 8)
-//      .. 32(w mod 8) + 31), and store them as fp16 (round to nearest, as __float2half in the
-//      reference) straight into a 128-byte-swizzled K-major shared-memory tile (two buffers);
-//   2. one elected thread issues tcgen05.mma kind::f16 (fp16 x fp16 -> fp32) for the two
-//      128-row halves against the PCA factor M (fp16, resident in shared memory for the whole
-//      kernel), accumulating dW in tensor memory; tcgen05.commit signals an mbarrier;
-//   3. warps 0-7 drain the TMEM lanes of their 32 paths with tcgen05.ld (32 columns = 32 time
-//      steps at a time) and feed the increments to the path consumer.
-// Generation of K-block kb+1 overlaps the MMA of K-block kb, and warps 8-15 generate the next
-// tile's first K-block while warps 0-7 drain this one.  Every mbarrier wait is bounded:
-// after the limit the CTA records MCQ_ERR_TIMEOUT in p.err, frees its TMEM and returns.
+// :1228-1229, :720-724).  Here one persistent, warp-specialised kernel does it per tile of 128
+// paths (one M = 128 MMA), with the PCA factor M (fp16, N x N) resident in shared memory:
+//   * 24 generator warps make the tile's scrambled-Sobol normals, 64 dimensions (one K-block) at
+//     a time: a K-block is eight work units of 32 paths x 32 dimensions, one per warp of a group
+//     of eight, and the three groups take every third K-block.  They store the normals as fp16
+//     (round to nearest, as __float2half in the reference) straight into a 128-byte-swizzled
+//     K-major stage of a four-stage ring and arrive on the stage's `full` barrier;
+//   * one issuer thread waits for a stage, issues tcgen05.mma kind::f16 (fp16 x fp16 -> fp32)
+//     against M, and releases the stage with tcgen05.commit on its `empty` barrier; after a
+//     tile's last K-block it commits the tile's accumulator;
+//   * the accumulator is double-buffered in tensor memory (2 x N columns): four drain warps (one
+//     per TMEM lane quarter) read their 32 paths' lanes with tcgen05.ld (32 time steps at a
+//     time), feed the increments to the path consumer and release the accumulator, so that a
+//     tile's drain overlaps the next tile's generation and MMA.
+// The normal generation bounds the kernel (the path consumer is a small fraction of the
+// instructions), so most warps generate: 4 drain + 24 generator warps + 1 issuer warp, 928
+// threads at up to 64 registers; 16 generators with 8 drain warps ran 19 % slower.
+// Every mbarrier wait is bounded: after the limit the CTA records MCQ_ERR_TIMEOUT in p.err, the
+// issuer waits (bounded) for its MMAs in flight, and the CTA frees its TMEM and returns.
 //
 // Supported sizes: N = D in {64, 128, 256} (K-blocks of 64, MMA N <= 256).
 #include <cuda_fp16.h>
@@ -24,10 +30,14 @@
 
 namespace mcq {
 
-constexpr int kPcaWarps = 8;                     // path-owning warps: 32 paths each, 256 per tile
-constexpr int kPcaGenWarps = 2 * kPcaWarps;       // all warps generate, half a K-block each
-constexpr int kPcaThreads = kPcaGenWarps * 32;
-constexpr int kABufBytes = 256 * 128;        // 256 rows x 64 fp16
+constexpr int kPcaDrainWarps = 4;            // warps 0-3: one per TMEM lane quarter
+constexpr int kPcaGenWarps = 24;             // warps 4-27: three groups of eight
+constexpr int kPcaGroups = kPcaGenWarps / 8;
+constexpr int kPcaIssuerWarp = kPcaDrainWarps + kPcaGenWarps;
+constexpr int kPcaThreads = (kPcaIssuerWarp + 1) * 32;
+constexpr int kPcaRows = 128;                // paths per tile: one M = 128 MMA
+constexpr int kPcaStages = 4;                // ring of K-block stages
+constexpr int kAStageBytes = kPcaRows * 128; // 128 rows x 64 fp16
 constexpr uint32_t kWaitLimit = 1u << 26;    // polls of an mbarrier before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
@@ -36,6 +46,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
 }
 
 // Bounded wait for completion of the phase with parity `parity`; returns false on timeout.
@@ -156,11 +170,16 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
     const int N = p.D;
     const int nkb = N >> 6;
     unsigned char* sB = sm;
-    unsigned char* sA0 = sm + N * N * 2;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sA0 + 2 * kABufBytes);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+    unsigned char* sA = sm + N * N * 2;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sA + kPcaStages * kAStageBytes);  // stage written
+    uint64_t* empty = full + kPcaStages;       // stage read by its MMAs
+    uint64_t* accfull = empty + kPcaStages;    // accumulator a holds a finished tile
+    uint64_t* accempty = accfull + 2;          // accumulator a drained
+    uint64_t* done = accempty + 2;             // every MMA issued has completed
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t ncols = (uint32_t)(2 * N);   // two 128-lane accumulators of N fp32 columns
+    const uint32_t ncols = (uint32_t)(2 * N);   // two accumulators of N fp32 columns
 
     // the PCA factor, row i = output step, K contiguous: 16-byte chunks into the swizzled layout
     {
@@ -173,8 +192,16 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
         }
     }
     if (tid == 0) {
-        mbar_init(smem_u32(&mbar[0]), 1);
-        mbar_init(smem_u32(&mbar[1]), 1);
+        for (int s = 0; s < kPcaStages; s++) {
+            mbar_init(smem_u32(&full[s]), 8 * 32);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(smem_u32(&accfull[a]), 1);
+            mbar_init(smem_u32(&accempty[a]), 4 * 32);
+        }
+        mbar_init(smem_u32(done), 1);
+        *s_fail = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -188,90 +215,125 @@ __global__ void __launch_bounds__(kPcaThreads, 1) k_pca(const __grid_constant__ 
     tc_fence_after();
     const uint32_t tbase = *tslot;
 
-    const uint32_t idesc = (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-    const uint32_t sB_addr = smem_u32(sB), sA_addr = smem_u32(sA0);
-    uint32_t phase[2] = {0u, 0u};
-    bool failed = false;
-
-    const int tiles_per_rep = (int)((p.G + 7) >> 3);
+    // Every role walks the same sequence: items blockIdx.x, + gridDim.x, ...; tiles [t_beg, t_end)
+    // of each item; q counts the CTA's tiles, K-block kb of tile q is the CTA's K-block q nkb + kb.
+    const int tiles_per_rep = (int)((p.G + 3) >> 2);
     const int n_items = p.n_items;
-    for (int item = blockIdx.x; item < n_items && !failed; item += gridDim.x) {
-        const int r = item / p.items_per_rep;
-        const int j = item - r * p.items_per_rep;
-        const int t_beg = j * p.gpi;
-        const int t_end = min(t_beg + p.gpi, tiles_per_rep);
-        const uint32_t* dr = p.dirs + (size_t)r * 33 * (size_t)N;
-        Acc<C::NST> acc;
-        acc.zero();
-        for (int t = t_beg; t < t_end && !failed; t++) {
-            const uint64_t h = p.g0 + (uint64_t)t * 8 + (uint64_t)(warp & 7);
-            const uint64_t n = h * 32 + (uint64_t)lane;
-            const int khalf = warp >> 3;   // which 32 of the K-block's 64 dimensions this warp makes
-            bool outstanding[2] = {false, false};
-            for (int kb = 0; kb < nkb; kb++) {
-                const int b = kb & 1;
-                unsigned char* A = sA0 + b * kABufBytes;
-                if (outstanding[b]) {   // the MMA that read this buffer two K-blocks ago
-                    const bool ok = mbar_wait(smem_u32(&mbar[b]), phase[b]);
-                    phase[b] ^= 1u;
-                    outstanding[b] = false;
-                    if (__syncthreads_or(!ok)) { failed = true; break; }
-                }
-                sobol_tile_to_A(dr, N, kb * 64 + 32 * khalf + lane, h, p.u_cap, A, (warp & 7) * 32, 32 * khalf + lane);
-                fence_proxy_async();
-                __syncthreads();
-                if (tid == 0) {
-                    tc_fence_after();
+    if (warp < kPcaDrainWarps) {
+        // ---- drain warps: every tile, tile q from accumulator q mod 2
+        const int quarter = warp;
+        const uint32_t tlane = tbase + ((uint32_t)(32 * quarter) << 16);
+        int q = 0;
+        bool stop = false;
+        for (int item = blockIdx.x; item < n_items && !stop; item += gridDim.x) {
+            const int r = item / p.items_per_rep;
+            const int j = item - r * p.items_per_rep;
+            const int t_beg = j * p.gpi;
+            const int t_end = min(t_beg + p.gpi, tiles_per_rep);
+            Acc<C::NST> acc;
+            acc.zero();
+            for (int t = t_beg; t < t_end; t++, q++) {
+                const int a = q & 1;
+                const uint32_t trow = tlane + (uint32_t)(a * N);
+                const bool ok = mbar_wait(smem_u32(&accfull[a]), (uint32_t)(q >> 1) & 1u);
+                if (!__all_sync(0xffffffffu, ok && !*s_fail)) { *s_fail = 1; stop = true; break; }
+                tc_fence_after();
+                const uint64_t n = (p.g0 + (uint64_t)t * 4 + (uint64_t)quarter) * 32 + (uint64_t)lane;
+                C cons;
+                cons.init(p);
+                if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
+                else cons.bind(r, n);
+                for (int c0 = 0; c0 < N; c0 += 32) {
+                    float v[32];
+                    tmem_ld32(trow + (uint32_t)c0, v);
 #pragma unroll
-                    for (int half = 0; half < 2; half++) {
-                        const uint32_t a0 = sA_addr + b * kABufBytes + half * (128 * 128);
-                        const uint32_t b0 = sB_addr + kb * (N * 128);
-                        const uint32_t d = tbase + (uint32_t)(half * N);
-#pragma unroll
-                        for (int ks = 0; ks < 4; ks++)
-                            mma_f16(d, sw128_desc(a0 + ks * 32), sw128_desc(b0 + ks * 32), idesc,
-                                    (kb | ks) != 0 ? 1u : 0u);
-                    }
-                    mma_commit(smem_u32(&mbar[b]));
+                    for (int i = 0; i < 32; i++) cons.step_dw(p, v[i], 0.f);
+                    cons.flush();
                 }
-                outstanding[b] = true;
+                tc_fence_before();   // TMEM reads done before the accumulator is released
+                mbar_arrive(smem_u32(&accempty[a]));
+                float y[C::NST];
+                cons.finish(p, y);
+                if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
             }
-            if (failed) break;
-            bool ok = true;
-            for (int b = 0; b < 2; b++) {
-                if (outstanding[b]) {
-                    ok = mbar_wait(smem_u32(&mbar[b]), phase[b]) && ok;
-                    phase[b] ^= 1u;
-                }
-            }
-            if (__syncthreads_or(!ok)) { failed = true; break; }
-            tc_fence_after();
-            if (warp >= kPcaWarps) {   // generators only: go on to the next tile's first K-block
-                tc_fence_before();
-                continue;
-            }
-            C cons;
-            cons.init(p);
-            if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
-            else cons.bind(r, n);
-            const uint32_t trow = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * N);
-            for (int c0 = 0; c0 < N; c0 += 32) {
-                float v[32];
-                tmem_ld32(trow + (uint32_t)c0, v);
-#pragma unroll
-                for (int i = 0; i < 32; i++) cons.step_dw(p, v[i], 0.f);
-                cons.flush();
-            }
-            float y[C::NST];
-            cons.finish(p, y);
-            if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
-            tc_fence_before();   // TMEM reads done before the next tile's first MMA overwrites it
+            if (!stop) acc.flush(p.partials + ((size_t)item * kPcaDrainWarps + warp) * C::NST, lane);
         }
-        if (warp < kPcaWarps) acc.flush(p.partials + ((size_t)item * kPcaWarps + warp) * C::NST, lane);
+    } else if (warp < kPcaIssuerWarp) {
+        // ---- generator warps: group grp (eight warps) makes the K-blocks jj with jj mod (groups) =
+        //      grp; warp gi makes unit (row group rg, dimension half hf) of each: rows 32 rg ..
+        //      32 rg + 31, dimensions 32 hf .. 32 hf + 31 of the K-block
+        const int gi = warp - kPcaDrainWarps;
+        const int rg = gi & 3, hf = (gi >> 2) & 1, grp = gi >> 3;
+        int q = 0;
+        bool stop = false;
+        for (int item = blockIdx.x; item < n_items && !stop; item += gridDim.x) {
+            const int r = item / p.items_per_rep;
+            const int j = item - r * p.items_per_rep;
+            const int t_beg = j * p.gpi;
+            const int t_end = min(t_beg + p.gpi, tiles_per_rep);
+            const uint32_t* dr = p.dirs + (size_t)r * 33 * (size_t)N;
+            for (int t = t_beg; t < t_end && !stop; t++, q++) {
+                const uint64_t h = p.g0 + (uint64_t)t * 4 + (uint64_t)rg;
+                for (int kb = 0; kb < nkb; kb++) {
+                    const int jj = q * nkb + kb;
+                    if (jj % kPcaGroups != grp) continue;
+                    const int s = jj % kPcaStages, u = jj / kPcaStages;
+                    if (u > 0) {   // the MMAs of this stage's previous K-block have read it
+                        const bool ok = mbar_wait(smem_u32(&empty[s]), (uint32_t)(u - 1) & 1u);
+                        if (!__all_sync(0xffffffffu, ok && !*s_fail)) { *s_fail = 1; stop = true; break; }
+                    }
+                    sobol_tile_to_A(dr, N, kb * 64 + 32 * hf + lane, h, p.u_cap, sA + s * kAStageBytes, 32 * rg,
+                                    32 * hf + lane);
+                    fence_proxy_async();   // generic-proxy stores visible to the tensor core's reads
+                    mbar_arrive(smem_u32(&full[s]));
+                }
+            }
+        }
+    } else if (lane == 0) {
+        // ---- the issuer thread
+        const uint32_t idesc = (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kPcaRows >> 4) << 24);
+        const uint32_t sB_addr = smem_u32(sB), sA_addr = smem_u32(sA);
+        int q = 0;
+        bool stop = false;
+        for (int item = blockIdx.x; item < n_items && !stop; item += gridDim.x) {
+            const int j = item - (item / p.items_per_rep) * p.items_per_rep;
+            const int t_beg = j * p.gpi;
+            const int t_end = min(t_beg + p.gpi, tiles_per_rep);
+            for (int t = t_beg; t < t_end && !stop; t++, q++) {
+                const int a = q & 1;
+                if (q >= 2 && (!mbar_wait(smem_u32(&accempty[a]), (uint32_t)((q >> 1) - 1) & 1u) || *s_fail)) {
+                    *s_fail = 1;
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tbase + (uint32_t)(a * N);
+                for (int kb = 0; kb < nkb; kb++) {
+                    const int jj = q * nkb + kb;
+                    const int s = jj % kPcaStages, u = jj / kPcaStages;
+                    if (!mbar_wait(smem_u32(&full[s]), (uint32_t)u & 1u) || *s_fail) {
+                        *s_fail = 1;
+                        stop = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = sA_addr + s * kAStageBytes, b0 = sB_addr + kb * (N * 128);
+#pragma unroll
+                    for (int ks = 0; ks < 4; ks++)
+                        mma_f16(d, sw128_desc(a0 + ks * 32), sw128_desc(b0 + ks * 32), idesc, (kb | ks) != 0 ? 1u : 0u);
+                    mma_commit(smem_u32(&empty[s]));
+                }
+                if (!stop) mma_commit(smem_u32(&accfull[a]));
+            }
+        }
+        // teardown: the commit tracks every MMA issued so far
+        mma_commit(smem_u32(done));
+        if (!mbar_wait(smem_u32(done), 0u)) *s_fail = 1;
     }
-    if (failed && tid == 0) atomicExch(p.err, MCQ_ERR_TIMEOUT_CODE);
+    __syncwarp();   // the issuer warp reconverges
     tc_fence_before();
     __syncthreads();
+    if (tid == 0 && *s_fail) atomicExch(p.err, MCQ_ERR_TIMEOUT_CODE);
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(ncols));
@@ -309,8 +371,9 @@ const void* lookup_pca(int model, int payoff, bool coupled, bool dump) {
     }
 }
 
-size_t pca_smem_bytes(int N) { return (size_t)N * N * 2 + 2 * kABufBytes + 64 + 1024; }
+size_t pca_smem_bytes(int N) { return (size_t)N * N * 2 + (size_t)kPcaStages * kAStageBytes + 256 + 1024; }
 int pca_threads() { return kPcaThreads; }
-int pca_warps() { return kPcaWarps; }
+int pca_warps() { return kPcaDrainWarps; }
+int pca_tile_paths() { return kPcaRows; }
 
 }  // namespace mcq

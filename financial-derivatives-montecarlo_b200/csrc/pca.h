@@ -7,9 +7,10 @@ namespace mcq {
 // Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
 constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
 
-const void* lookup_pca(int model, int payoff, bool coupled, bool dump);
-size_t pca_smem_bytes(int N);
-int pca_threads();
-int pca_warps();
+const void* lookup_pca(int model, int payoff, bool coupled, bool dump);   // nullptr: unsupported
+size_t pca_smem_bytes(int N);   // dynamic shared memory of a launch
+int pca_threads();      // block size
+int pca_warps();        // per-warp records per work item
+int pca_tile_paths();   // paths per tile
 
 }  // namespace mcq

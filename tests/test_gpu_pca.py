@@ -70,3 +70,60 @@ def test_pca_qmc_driver_and_mlqmc(gpu, orc):
     assert abs(q["price"] - bs) < 4 * q["std_error"] + 5e-3 / np.sqrt(2), q
     for h in lst:
         h.close()
+
+
+def _lv_model(gpu, name):
+    if name == "dupire":
+        return gpu.dupire(100.0, 0.05, 0.2, 0.5, 0.7, 1.0)
+    K = np.linspace(50, 150, 64)
+    t = np.linspace(0, 2, 32)
+    g = 0.2 + 0.1 * np.exp(-(K[None, :] / 100 - 1) ** 2 / 0.05) * (1 + 0.5 * t[:, None])
+    return gpu.localvol_grid(K, t, g, 100.0, 0.05, 1.0)
+
+
+@pytest.mark.parametrize("model", ["dupire", "lv"])
+@pytest.mark.parametrize("N", [64, 128])
+def test_pca_pass_local_vol_models_vs_oracle(gpu, orc, model, N):
+    """The tensor-core pass with the parametric and the grid local-volatility models."""
+    m, p = _lv_model(gpu, model), gpu.asian(100.0)
+    pca = gpu.pca_create(N, 1.0)
+    R, Np, off = 2, 1500, 21
+    g = gpu.qmc_pass(m, p, N, noise=gpu.PCA, pca=pca, salt_base=17, R=R, offset=off, n_points=Np)
+    o = orc.qmc_sums(m, p, N, orc.noise(orc.T.PCA, N, 1.0), salt_base=17, R=R, offset=off, N=Np)
+    for r in range(R):
+        assert abs(g[r, 0] / Np - o[r, 0] / Np) < 3e-4 * (1 + abs(o[r, 0] / Np)), (r, g[r], o[r])
+    pca.close()
+
+
+@pytest.mark.parametrize("model", ["gbm", "dupire"])
+@pytest.mark.parametrize("n_fine,M", [(64, 2), (128, 4), (256, 2)])
+def test_pca_coupled_level_vs_oracle(gpu, orc, model, n_fine, M):
+    """A coupled MLQMC level (fine path on the tensor-core PCA increments, coarse path on their
+    M-step sums) against the oracle's level sums."""
+    m = _lv_model(gpu, "dupire") if model == "dupire" else gpu.gbm(100.0, 0.05, 0.2, 1.0)
+    p = gpu.european(100.0, 0.05, 1.0)
+    pca = gpu.pca_create(n_fine, 1.0)
+    R, Np = 2, 1024
+    g = gpu.level_pass(m, p, n_fine, M, noise=gpu.PCA, pca=pca, use_sobol=True, salt_base=90, R=R, offset=3,
+                       n_points=Np)
+    o = orc.level_sums(m, p, n_fine, M, orc.noise(orc.T.PCA, n_fine, 1.0), use_sobol=True, salt_base=90, R=R,
+                       offset=3, N=Np)
+    for r in range(R):
+        for k in (0, 2):
+            assert abs(g[r, k] / Np - o[r, k] / Np) < 4e-4 * (1 + abs(o[r, k] / Np)), (r, k, g[r], o[r])
+    pca.close()
+
+
+def test_pca_ragged_ranges_add_up(gpu):
+    """A range split at points that are not multiples of the 128-path tile gives the sums of the
+    whole range: every path is counted once whatever the tiles, work items and TMEM accumulator
+    turns.  The tolerance covers the FP32 compensated per-lane sums (one path is 1e-5 of the
+    total here)."""
+    m, p = gpu.gbm(100.0, 0.03, 0.25, 1.0), gpu.asian(100.0)
+    pca = gpu.pca_create(128, 1.0)
+    kw = dict(noise=gpu.PCA, pca=pca, salt_base=42, R=3)
+    whole = gpu.qmc_pass(m, p, 128, offset=5, n_points=100001, **kw)
+    parts = sum(gpu.qmc_pass(m, p, 128, offset=a, n_points=b - a, **kw)
+                for a, b in [(5, 133), (133, 134), (134, 50001), (50001, 100006)])
+    np.testing.assert_allclose(parts, whole, rtol=2e-6)
+    pca.close()
