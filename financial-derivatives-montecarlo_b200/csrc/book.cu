@@ -80,6 +80,19 @@ constexpr int kBookLsFloats = kMaxBasket * kMaxBasket;
 constexpr int kBookAssetFloats = 4 * kMaxBasket;   // sigma, S0, weight, weight / S0 per asset
 constexpr int kBookWarpFloats = 1024 + kBookLsFloats + kBookAssetFloats + 2 * kBookNST;
 
+// A float4 of shared memory, read at every use.  The Cholesky rows are loop-invariant and the
+// compiler otherwise keeps the factor in registers across the chunk; for baskets of up to four
+// assets, reading it at every step lets the class run at 64 registers (four CTAs per SM instead
+// of three: 1.08-1.17x).  The wider classes keep the cached factor (re-reading it and a
+// tighter budget made d = 5-8 3-7 % slower and d = 9-12 no faster).
+__device__ __forceinline__ float4 lds4(const float4* p) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"((unsigned)__cvta_generic_to_shared(p)));
+    return v;
+}
+
 // The coupled basket pair of one path for a basket of exactly D assets: the correlated Euler
 // step S + S (mu h + sigma dW) with dW = L x, x = z sqrt(h), coarse steps on the summed fine
 // increments every M fine steps, the call on the weighted basket and d payoff / d S0_a =
@@ -107,7 +120,7 @@ struct BookPath {
             float dw = 0.f;
 #pragma unroll
             for (int j4 = 0; j4 <= q / 4; j4++) {
-                const float4 v = L4[(q * DP) / 4 + j4];
+                const float4 v = (D <= 4) ? lds4(L4 + (q * DP) / 4 + j4) : L4[(q * DP) / 4 + j4];
                 dw = fmaf(v.x, x[4 * j4], dw);
                 if (4 * j4 + 1 <= q) dw = fmaf(v.y, x[4 * j4 + 1], dw);
                 if (4 * j4 + 2 <= q) dw = fmaf(v.z, x[4 * j4 + 2], dw);
@@ -344,37 +357,61 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
     }
 }
 
-// Per slice: replica sums from its chunk records in chunk order, then the mean of the replica
-// means of dY, their sample variance and the mean per-asset delta.  One warp per slice, one
-// lane per statistic.
+// Per slice: the replica sums of its chunk records, then the mean of the replica means of dY,
+// their sample variance and the mean per-asset delta.  One CTA per slice and one warp per
+// replica: lane l adds the records of chunks l, l + 32, l + 64, ... in that order, the 32 lane
+// sums are combined by an xor butterfly (offsets 16, 8, 4, 2, 1), and warp 0 forms the slice
+// statistics from the R replica sums in replica order.  book_level_sums restates the same
+// order on the host.
+constexpr int kFinStats = 1 + kMaxBasket;   // dY and the deltas: record entries 0 and 4 ..
 __global__ void k_book_fin(const __grid_constant__ BookArgs a) {
-    const int lane = threadIdx.x & 31;
+    __shared__ double rs[kBookMaxR][kFinStats];
+    const int lane = threadIdx.x & 31, rw = threadIdx.x >> 5;
     const int n_specs = a.hdr[0];
-    const int wpb = blockDim.x >> 5;
-    const int st = (lane == 0) ? 0 : (lane <= kMaxBasket ? 3 + lane : -1);   // dY or a delta
-    for (int s = blockIdx.x * wpb + (threadIdx.x >> 5); s < n_specs; s += gridDim.x * wpb) {
-        if (st < 0) continue;
+    for (int s = blockIdx.x; s < n_specs; s += gridDim.x) {
         const BookSpec sp = a.specs[s];
-        double rep[kBookMaxR];
-        double m = 0.0;
-        for (int r = 0; r < a.R; r++) {
-            double v = 0.0;
-            for (int j = 0; j < sp.cpr; j++) v += a.records[(size_t)(sp.chunk0 + r * sp.cpr + j) * kBookNST + st];
-            rep[r] = v / (double)sp.n_points;
-            m += rep[r];
+        if (rw < a.R) {
+            double v[kFinStats];
+#pragma unroll
+            for (int k = 0; k < kFinStats; k++) v[k] = 0.0;
+            for (int j = lane; j < sp.cpr; j += 32) {
+                const double* rec = a.records + (size_t)(sp.chunk0 + rw * sp.cpr + j) * kBookNST;
+                v[0] += rec[0];
+#pragma unroll
+                for (int k = 1; k < kFinStats; k++) v[k] += rec[3 + k];
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+                for (int k = 0; k < kFinStats; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < kFinStats; k++) rs[rw][k] = v[k];
+            }
         }
-        m /= a.R;
-        double* o = a.out + (size_t)s * kBookOut;
-        if (lane == 0) {
-            double v = 0.0;
-            // separate roundings (no fused multiply-add), so that a host restatement in IEEE
-            // double gives the same bits
-            for (int r = 0; r < a.R; r++) v = __dadd_rn(v, __dmul_rn(rep[r] - m, rep[r] - m));
-            o[0] = m;
-            o[1] = a.R > 1 ? v / (a.R - 1) : 0.0;
-        } else {
-            o[1 + lane] = m;
+        __syncthreads();
+        if (rw == 0 && lane < kFinStats) {
+            double rep[kBookMaxR];
+            double m = 0.0;
+            for (int r = 0; r < a.R; r++) {
+                rep[r] = rs[r][lane] / (double)sp.n_points;
+                m += rep[r];
+            }
+            m /= a.R;
+            double* o = a.out + (size_t)s * kBookOut;
+            if (lane == 0) {
+                double v = 0.0;
+                // separate roundings (no fused multiply-add), so that a host restatement in IEEE
+                // double gives the same bits
+                for (int r = 0; r < a.R; r++) v = __dadd_rn(v, __dmul_rn(rep[r] - m, rep[r] - m));
+                o[0] = m;
+                o[1] = a.R > 1 ? v / (a.R - 1) : 0.0;
+            } else {
+                o[1 + lane] = m;
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -408,7 +445,7 @@ size_t book_smem() { return (size_t)kWarpsPerBlock * kBookWarpFloats * sizeof(fl
 using BookFn = void (*)(BookArgs);
 BookFn book_fn(int cls) {
     switch (cls) {
-        case 0: return k_book<0, 3>;
+        case 0: return k_book<0, 4>;
         case 1: return k_book<1, 2>;
         case 2: return k_book<2, 2>;
         default: return k_book<3, 2>;
@@ -680,7 +717,7 @@ struct BookRunner {
     }
     void launch_fin(const BookArgs& a, int grid, cudaStream_t st_) {
         void* argv[] = {(void*)&a};
-        MCQ_CUDA(cudaLaunchKernel((const void*)k_book_fin, dim3(grid), dim3(256), argv, 0, st_));
+        MCQ_CUDA(cudaLaunchKernel((const void*)k_book_fin, dim3(grid), dim3(32 * a.R), argv, 0, st_));
     }
 
     // ---- batched: one graph per book, replayed once per round
@@ -838,11 +875,22 @@ void book_level_sums(const mcq_book_option& opt, const mcq_mlmc_cfg& ml, const m
     MCQ_CUDA(cudaMemcpyAsync(rec.data(), s.records.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.stream));
     MCQ_CUDA(cudaStreamSynchronize(s.stream));
     engine().launches += 1;
+    // the summation order of k_book_fin: per lane l the chunks l, l + 32, ..., then the xor butterfly
+    const int cpr = one[0].cpr;
     for (int r = 0; r < b.R; r++)
         for (int q = 0; q < kBookNST; q++) {
-            double v = 0.0;
-            for (int j = 0; j < one[0].cpr; j++) v += rec[(size_t)(r * one[0].cpr + j) * kBookNST + q];
-            sums_host[(size_t)r * kBookNST + q] = v;
+            double part[32];
+            for (int l = 0; l < 32; l++) {
+                double v = 0.0;
+                for (int j = l; j < cpr; j += 32) v += rec[(size_t)(r * cpr + j) * kBookNST + q];
+                part[l] = v;
+            }
+            for (int off = 16; off > 0; off >>= 1) {
+                double nxt[32];
+                for (int l = 0; l < 32; l++) nxt[l] = part[l] + part[l ^ off];
+                std::memcpy(part, nxt, sizeof(part));
+            }
+            sums_host[(size_t)r * kBookNST + q] = part[0];
         }
 }
 
