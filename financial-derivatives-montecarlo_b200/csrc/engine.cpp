@@ -359,10 +359,16 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
 
     const void* fn = a.dump ? lookup_misc(a.gen, a.noise, a.est, k.model, nb, true)
                             : lookup_pass(a.gen, a.noise, a.est, k.model, a.p->kind, nb);
+    // short raw-ordered Sobol paths: 32 / D path groups per tile instead of one
+    const void* packed = nullptr;
+    if (!a.dump && a.gen == GEN_SOBOL && a.noise == NOISE_RAW && D <= 16 &&
+        (a.est == EST_PLAIN || a.est == EST_COUPLED))
+        packed = lookup_sobol_packed(k.model, a.p->kind, a.est == EST_COUPLED);
+    if (packed) fn = packed;
     // launch variant: MCQ_TUNE=<v> forces one; otherwise the autotuner picks per family
     int variant = 0;
     TuneState* trial = nullptr;
-    const int nvar = a.dump ? 1 : n_variants(a.gen, a.noise, a.est, k.model);
+    const int nvar = (a.dump || packed) ? 1 : n_variants(a.gen, a.noise, a.est, k.model);
     if (nvar > 1) {
         const char* force = std::getenv("MCQ_TUNE");
         if (force) {
@@ -418,6 +424,10 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     const uint64_t G = ((a.offset + a.n_points - 1) >> 5) - g0 + 1;
     uint64_t gpi = (G * (uint64_t)a.R + kTargetItems - 1) / kTargetItems;
     if (gpi < 1) gpi = 1;
+    if (packed) {   // whole tiles of 32 / D groups per item
+        const uint64_t Q = (uint64_t)(32 / D);
+        gpi = (gpi + Q - 1) / Q * Q;
+    }
     const uint64_t ipr = (G + gpi - 1) / gpi;
     MCQ_REQUIRE(ipr * (uint64_t)a.R < (1ull << 31), MCQ_ERR_RANGE, "too many work items");
     k.R = a.R;

@@ -13,7 +13,9 @@
 namespace mcq {
 
 enum Gen : int { GEN_SOBOL = 0, GEN_PHILOX = 1 };
-enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2 };
+// NOISE_PACKED: raw ordering for paths of at most 16 normals, 32 / D path groups per Sobol tile
+// (an engine-internal choice, never requested through the API)
+enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3 };
 enum ModelK : int { MOD_GBM = 0, MOD_HESTON = 1, MOD_DUPIRE = 2, MOD_MULTI = 3, MOD_LVGRID = 4, MOD_BASKET = 5 };
 enum PayK : int { PAY_EUR = 0, PAY_ASIAN = 1, PAY_GEOM = 2, PAY_LOOKBACK = 3, PAY_UPOUT = 4, PAY_BASKET = 5, PAY_DOWNOUT = 6 };
 enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE = 3, EST_IS = 4 };

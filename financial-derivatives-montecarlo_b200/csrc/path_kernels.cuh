@@ -900,18 +900,47 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ?
         AccWarp<C::NST> wacc;
         if constexpr (WACC) wacc.bind(wrec, lane);
         else acc.zero();
-        for (uint64_t h = gb; h < ge; h++) {
-            const uint64_t n = h * 32 + (uint64_t)lane;
-            C cons;
-            cons.init(p);
-            if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
-            else cons.bind(r, n);
-            run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane);
-            float y[C::NST];
-            cons.finish(p, y);
-            const bool valid = n >= p.offset && n < p.offset + p.n_points;
-            if constexpr (WACC) wacc.add(y, valid, lane);
-            else if (valid) acc.add(y);
+        if constexpr (NOISE == NOISE_PACKED) {
+            // Paths of D <= 16 normals: one Sobol tile holds Q = 32 / D groups (lane j makes
+            // dimension j mod D of group h + j / D), and each lane then runs its Q paths from the
+            // transposed tile.  The normals and the order of the paths are those of the
+            // one-group-per-tile loop below; only the idle lanes of its tiles are put to work.
+            const int D = p.D, Q = 32 / D;
+            const int qj = lane / D, dj = lane - qj * D;
+            for (uint64_t h = gb; h < ge; h += (uint64_t)Q) {
+                const uint64_t hl = h + (uint64_t)qj;
+                sobol_tile(dr, p.dstride, dj, qj < Q && hl < ge, hl, p.u_cap, buf, lane);
+                __syncwarp();
+                const int nq = (int)min((uint64_t)Q, ge - h);
+                for (int q = 0; q < nq; q++) {
+                    const uint64_t n = (h + (uint64_t)q) * 32 + (uint64_t)lane;
+                    C cons;
+                    cons.init(p);
+                    cons.bind(r, n);
+                    float z[32];
+#pragma unroll
+                    for (int c = 0; c < 32; c++) z[c] = (c < 16 && c < D) ? buf[swz(lane, q * D + c)] : 0.f;
+                    cons.tile(p, z, D);
+                    float y[C::NST];
+                    cons.finish(p, y);
+                    if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
+                }
+                __syncwarp();
+            }
+        } else {
+            for (uint64_t h = gb; h < ge; h++) {
+                const uint64_t n = h * 32 + (uint64_t)lane;
+                C cons;
+                cons.init(p);
+                if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
+                else cons.bind(r, n);
+                run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane);
+                float y[C::NST];
+                cons.finish(p, y);
+                const bool valid = n >= p.offset && n < p.offset + p.n_points;
+                if constexpr (WACC) wacc.add(y, valid, lane);
+                else if (valid) acc.add(y);
+            }
         }
         if constexpr (WACC) wacc.flush(p.partials + (size_t)item * C::NST, lane);
         else acc.flush(p.partials + (size_t)item * C::NST, lane);
