@@ -162,6 +162,21 @@ def test_launch_variants_are_bit_identical(gpu, model, pay):
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
+@pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("heston", "lookback"), ("dupire", "eur")])
+def test_coupled_launch_variants_are_bit_identical(gpu, model, pay):
+    """The coupled MLMC / MLQMC level pass under its two register budgets."""
+    import os
+    m, p = make_model(gpu, model), make_payoff(gpu, pay)
+    out = []
+    try:
+        for v in ("0", "1"):
+            os.environ["MCQ_TUNE"] = v
+            out.append(gpu.level_pass(m, p, 64, 4, use_sobol=True, salt_base=42, R=4, offset=3, n_points=50000))
+    finally:
+        os.environ.pop("MCQ_TUNE", None)
+    assert np.array_equal(out[0], out[1])
+
+
 @pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("dupire", "eur")])
 def test_bridge_launch_variants_are_bit_identical(gpu, model, pay):
     import os
