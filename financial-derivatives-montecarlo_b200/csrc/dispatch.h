@@ -12,6 +12,7 @@ const void* lookup_sobol_raw_plain_b5(int model, int payoff);   // 48-register v
 const void* lookup_sobol_raw_coupled(int model, int payoff);
 const void* lookup_sobol_raw_coupled_b4(int model, int payoff);   // 64-register variant
 const void* lookup_sobol_packed(int model, int payoff, bool coupled);   // raw, D <= 16 (NOISE_PACKED)
+const void* lookup_assist(int gen, int model, int payoff, bool coupled);  // raw, few long paths (NOISE_ASSIST)
 const void* lookup_sobol_bb(int model, int payoff, bool coupled);
 const void* lookup_sobol_bb_b3(int model, int payoff);          // 3-CTA (80-register) variant
 const void* lookup_sobol_pca_small(int model, int payoff, bool coupled);   // N <= 32

@@ -210,6 +210,7 @@ void run_mlmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_mlm
         double* h = (double*)w.hsums.ensure(4 * sizeof(double));
         MCQ_CUDA(cudaMemcpyAsync(h, dsum[l], 4 * sizeof(double), cudaMemcpyDeviceToHost, w.stream));   // first 4 stats
         MCQ_CUDA(cudaStreamSynchronize(w.stream));
+        check_err_word(w);
         return std::vector<double>(h, h + 4);
     };
 
@@ -351,6 +352,7 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
         double* h = (double*)w.hsums.ensure((size_t)R * ns * sizeof(double));
         MCQ_CUDA(cudaMemcpyAsync(h, dsum[l], (size_t)R * ns * sizeof(double), cudaMemcpyDeviceToHost, w.stream));
         MCQ_CUDA(cudaStreamSynchronize(w.stream));
+        check_err_word(w);
         double mm = 0.0;
         for (int r = 0; r < R; r++) mm += h[ns * r] / n;
         mm /= R;

@@ -365,10 +365,19 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
         (a.est == EST_PLAIN || a.est == EST_COUPLED))
         packed = lookup_sobol_packed(k.model, a.p->kind, a.est == EST_COUPLED);
     if (packed) fn = packed;
+    // few, long raw-ordered paths (fewer 32-path groups than 8 warps per SM): helper warps
+    // generate each path-owning warp's normals
+    const void* assist = nullptr;
+    if (!a.dump && !packed && a.noise == NOISE_RAW && D >= 64 && (a.est == EST_PLAIN || a.est == EST_COUPLED)) {
+        const uint64_t groups = (((a.offset + a.n_points - 1) >> 5) - (a.offset >> 5) + 1) * (uint64_t)a.R;
+        if (groups < (uint64_t)E.sm_count * 8)
+            assist = lookup_assist(a.gen, k.model, a.p->kind, a.est == EST_COUPLED);
+    }
+    if (assist) fn = assist;
     // launch variant: MCQ_TUNE=<v> forces one; otherwise the autotuner picks per family
     int variant = 0;
     TuneState* trial = nullptr;
-    const int nvar = (a.dump || packed) ? 1 : n_variants(a.gen, a.noise, a.est, k.model);
+    const int nvar = (a.dump || packed || assist) ? 1 : n_variants(a.gen, a.noise, a.est, k.model);
     if (nvar > 1) {
         const char* force = std::getenv("MCQ_TUNE");
         if (force) {
@@ -459,11 +468,18 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
 
     const int skel = (a.noise == NOISE_BB && D > 32) ? ((D >> 5) + 1) * 32 : 0;
     const int accf = (!a.dump && a.est == EST_COUPLED && k.model == MOD_BASKET) ? ((2 * nst + 3) & ~3) : 0;
-    const size_t smem = (size_t)kWarpsPerBlock * (1024 + skel + accf) * sizeof(float);
+    const size_t smem = assist ? (size_t)kAssistTeams * kAssistTeamBytes
+                               : (size_t)kWarpsPerBlock * (1024 + skel + accf) * sizeof(float);
     KernelInfo& ki = kernel_info(fn, smem);
-    long long blocks = ((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int items_per_block = assist ? kAssistTeams : kWarpsPerBlock;
+    long long blocks = ((long long)k.n_items + items_per_block - 1) / items_per_block;
     blocks = std::min<long long>(blocks, (long long)ki.blocks_per_sm * E.sm_count);
     blocks = std::max<long long>(blocks, 1);
+    if (assist) {
+        k.err = (int*)ws.err.ensure(sizeof(int));
+        MCQ_CUDA(cudaMemsetAsync(k.err, 0, sizeof(int), ws.stream));
+        ws.err_armed = true;
+    }
     void* args[] = {&k};
     if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[variant][0], ws.stream));
     MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kThreads), args, smem, ws.stream));
@@ -528,7 +544,7 @@ void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out)
 }
 
 // A bounded device wait that gave up leaves MCQ_ERR_TIMEOUT in the workspace's error word.
-static void check_err_word(Workspace& ws) {
+void check_err_word(Workspace& ws) {
     if (!ws.err_armed) return;
     int h = 0;
     MCQ_CUDA(cudaMemcpy(&h, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost));

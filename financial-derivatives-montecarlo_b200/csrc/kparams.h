@@ -15,7 +15,12 @@ namespace mcq {
 enum Gen : int { GEN_SOBOL = 0, GEN_PHILOX = 1 };
 // NOISE_PACKED: raw ordering for paths of at most 16 normals, 32 / D path groups per Sobol tile
 // (an engine-internal choice, never requested through the API)
-enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3 };
+// NOISE_ASSIST: raw ordering for passes with few, long paths: each path-owning warp is fed its
+// normal tiles by three helper warps (engine-internal as well)
+enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3, NOISE_ASSIST = 4 };
+
+// Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
+constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
 enum ModelK : int { MOD_GBM = 0, MOD_HESTON = 1, MOD_DUPIRE = 2, MOD_MULTI = 3, MOD_LVGRID = 4, MOD_BASKET = 5 };
 enum PayK : int { PAY_EUR = 0, PAY_ASIAN = 1, PAY_GEOM = 2, PAY_LOOKBACK = 3, PAY_UPOUT = 4, PAY_BASKET = 5, PAY_DOWNOUT = 6 };
 enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE = 3, EST_IS = 4 };
@@ -25,6 +30,13 @@ constexpr int kThreads = kWarpsPerBlock * 32;
 constexpr int kMaxBasket = 16;          // register-resident basket width
 constexpr int kMinBlocks = 3;           // resident CTAs per SM the register budget is set for
 constexpr int kMaxStats = 8;
+// Assisted passes (NOISE_ASSIST): per owner warp, three helper warps and a ring of four 32 x 32
+// normal tiles with a `full` and an `empty` mbarrier per slot.
+constexpr int kAssistSlots = 4;
+constexpr int kAssistHelpers = 3;
+constexpr int kAssistTeam = 1 + kAssistHelpers;              // warps per owner
+constexpr int kAssistTeams = kWarpsPerBlock / kAssistTeam;   // owners per block
+constexpr int kAssistTeamBytes = kAssistSlots * 1024 * 4 + 2 * kAssistSlots * 8;
 
 struct KParams {
     // ---- geometry

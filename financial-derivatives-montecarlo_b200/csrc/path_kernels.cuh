@@ -868,6 +868,114 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
     }
 }
 
+// ------------------------------------------------------------------ assisted passes
+
+// A pass with few 32-path groups and long paths leaves most of the GPU idle: each warp walks its
+// paths' whole step sequence alone, and the generation of its normals stalls the sequential
+// path arithmetic it cannot overlap with.  Assisted passes give every path-owning warp three
+// helper warps that generate its normal tiles ahead into a four-slot shared-memory ring; the
+// owner reads each tile (its own row) and runs the consumer.  The normals, the consumer and the
+// work items are those of the plain loop, so the sums are the same bits.  Every wait is bounded;
+// a warp that gives up records MCQ_ERR_TIMEOUT in p.err and stops.
+constexpr uint32_t kAssistWaitLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t asst_addr(const void* ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void asst_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(asst_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool asst_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = asst_addr(bar);
+    for (uint32_t i = 0; i < kAssistWaitLimit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred q;\n mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, q;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int GEN, class C>
+__device__ __forceinline__ void assisted_pass(const KParams& p, unsigned char* smem) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int team = wib / kAssistTeam, role = wib - team * kAssistTeam;   // role 0 owns the paths
+    float* ring = reinterpret_cast<float*>(smem + team * kAssistTeamBytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring + kAssistSlots * 1024);
+    uint64_t* empty = full + kAssistSlots;
+    if (lane == 0 && role == 0) {
+        for (int s = 0; s < kAssistSlots; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asst_addr(&full[s])), "r"(32));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asst_addr(&empty[s])), "r"(32));
+        }
+    }
+    __syncthreads();
+    const int D = p.D, T = (D + 31) >> 5;   // tiles per path
+    const uint64_t gend_all = p.g0 + p.G;
+    const int total_teams = gridDim.x * kAssistTeams;
+    uint32_t u = 0;   // the team's tile sequence number: tile t of group h in item order
+    bool stop = false;
+    for (int item = blockIdx.x * kAssistTeams + team; item < p.n_items && !stop; item += total_teams) {
+        const int r = item / p.items_per_rep;
+        const int j = item - r * p.items_per_rep;
+        const uint64_t gb = p.g0 + (uint64_t)j * (uint64_t)p.gpi;
+        const uint64_t ge = min(gb + (uint64_t)p.gpi, gend_all);
+        if (role == 0) {
+            Acc<C::NST> acc;
+            acc.zero();
+            for (uint64_t h = gb; h < ge && !stop; h++) {
+                const uint64_t n = h * 32 + (uint64_t)lane;
+                C cons;
+                cons.init(p);
+                cons.bind(r, n);
+                for (int t = 0; t < T; t++, u++) {
+                    const int s = (int)(u % kAssistSlots);
+                    const bool ok = asst_wait(&full[s], (u / kAssistSlots) & 1u);
+                    if (!__all_sync(0xffffffffu, ok)) { stop = true; break; }
+                    float z[32];
+                    read_row(ring + s * 1024, lane, z);
+                    asst_arrive(&empty[s]);
+                    cons.tile(p, z, min(32, D - 32 * t));
+                }
+                if (stop) break;
+                float y[C::NST];
+                cons.finish(p, y);
+                if (n >= p.offset && n < p.offset + p.n_points) acc.add(y);
+            }
+            if (!stop) acc.flush(p.partials + (size_t)item * C::NST, lane);
+        } else {
+            const uint32_t* dr = (GEN == GEN_SOBOL) ? p.dirs + (size_t)r * 33 * (size_t)p.dstride : nullptr;
+            const uint32_t stream = p.stream_base + (uint32_t)r;
+            for (uint64_t h = gb; h < ge && !stop; h++) {
+                for (int t = 0; t < T; t++, u++) {
+                    if ((int)(u % kAssistHelpers) != role - 1) continue;
+                    const int s = (int)(u % kAssistSlots);
+                    const uint32_t use = u / kAssistSlots;
+                    if (use > 0) {   // the owner has read this slot's previous tile
+                        const bool ok = asst_wait(&empty[s], (use - 1) & 1u);
+                        if (!__all_sync(0xffffffffu, ok)) { stop = true; break; }
+                    }
+                    float* b = ring + s * 1024;
+                    if constexpr (GEN == GEN_SOBOL) {
+                        sobol_tile(dr, p.dstride, 32 * t + lane, 32 * t + lane < D, h, p.u_cap, b, lane);
+                    } else {
+                        float z[32];
+                        philox_tile(p.seed, stream, h * 32 + (uint64_t)lane, t, z);
+                        float4* row = reinterpret_cast<float4*>(b + lane * 32);
+#pragma unroll
+                        for (int c = 0; c < 8; c++)
+                            row[c ^ (lane & 7)] = make_float4(z[4 * c], z[4 * c + 1], z[4 * c + 2], z[4 * c + 3]);
+                    }
+                    asst_arrive(&full[s]);
+                }
+            }
+        }
+    }
+    if (stop && lane == 0) atomicExch(p.err, MCQ_ERR_TIMEOUT_CODE);
+}
+
 // MINB: resident CTAs per SM the register budget is set for (0: 2 for the bridge, whose
 // window keeps 33 W values live, kMinBlocks otherwise).  Variants differ only in register
 // allocation and scheduling, never in arithmetic, so they produce identical sums.
@@ -880,6 +988,10 @@ template <int GEN, int NOISE, class C, int MINB = 0>
 __global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ? 2 : kMinBlocks))
     k_pass(const __grid_constant__ KParams p) {
     extern __shared__ float4 smem4[];
+    if constexpr (NOISE == NOISE_ASSIST) {
+        assisted_pass<GEN, C>(p, reinterpret_cast<unsigned char*>(smem4));
+        return;
+    }
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     constexpr bool WACC = warp_acc_of<C>::value;
     const int skel_floats = (NOISE == NOISE_BB && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;

@@ -2,10 +2,9 @@
 #pragma once
 #include <cstddef>
 
-namespace mcq {
+#include "kparams.h"
 
-// Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
-constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
+namespace mcq {
 
 const void* lookup_pca(int model, int payoff, bool coupled, bool dump);   // nullptr: unsupported
 size_t pca_smem_bytes(int N);   // dynamic shared memory of a launch
