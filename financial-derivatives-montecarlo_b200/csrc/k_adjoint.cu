@@ -112,23 +112,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             for (int d0 = 0; d0 < N; d0 += 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
-                float z[32];
-                read_row(buf, lane, z);
-                __syncwarp();
-#pragma unroll
+                // the step loops read this lane's row of the tile from shared memory and stay
+                // mostly rolled: fully unrolled, the sweeps overflowed the instruction cache
+#pragma unroll 4
                 for (int i = 0; i < 32; i++) {
                     const int k = d0 + i;
                     if ((i & (kCk - 1)) == 0) ck[(k / kCk) * 32 + lane] = S;
                     float dsS, dsP;
                     LvEval lv;
                     const float sig = local_sigma<MOD>(p, S, (float)k * h, &dsS, &dsP, &lv);
-                    S = fmaf(S, fmaf(sig, z[i] * sqh, muh), S);
+                    S = fmaf(S, fmaf(sig, buf[swz(lane, i)] * sqh, muh), S);
                     if constexpr (PAY == PAY_ASIAN) ts += S;
                     if constexpr (PAY == PAY_LOOKBACK) {
                         if (S < mn) { mn = S; kmin = k + 1; }
                     }
                 }
                 if constexpr (PAY == PAY_ASIAN) { kadd(tot, comp, ts); ts = 0.f; }
+                __syncwarp();
             }
             // payoff and its direct derivatives
             float P, g_all = 0.f, Sbar;
@@ -149,26 +149,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
-                float z[32];
-                read_row(buf, lane, z);
-                __syncwarp();
-#pragma unroll
+#pragma unroll 1
                 for (int s = 1; s >= 0; s--) {
                     const int k0 = d0 + s * kCk;
                     float Sr = ck[(k0 / kCk) * 32 + lane];
-#pragma unroll
+#pragma unroll 4
                     for (int i = 0; i < kCk; i++) {
                         seg[i * 32 + lane] = Sr;
                         float dsS, dsP;
                         LvEval lv;
                         const float sig = local_sigma<MOD>(p, Sr, (float)(k0 + i) * h, &dsS, &dsP, &lv);
-                        Sr = fmaf(Sr, fmaf(sig, z[s * kCk + i] * sqh, muh), Sr);
+                        Sr = fmaf(Sr, fmaf(sig, buf[swz(lane, s * kCk + i)] * sqh, muh), Sr);
                     }
-#pragma unroll
+#pragma unroll 4
                     for (int i = kCk - 1; i >= 0; i--) {
                         const int k = k0 + i;
                         const float Sk = seg[i * 32 + lane];
-                        const float dw = z[s * kCk + i] * sqh;
+                        const float dw = buf[swz(lane, s * kCk + i)] * sqh;
                         float dsS, dsP;
                         LvEval lv;
                         const float sig = local_sigma<MOD>(p, Sk, (float)k * h, &dsS, &dsP, &lv);
@@ -193,6 +190,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                         Sbar = fmaf(Sbar, dS1, direct);
                     }
                 }
+                __syncwarp();
             }
             float rho = mubar;
             if constexpr (PAY == PAY_EUR) rho -= p.pay_T * P;
