@@ -365,10 +365,12 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
         (a.est == EST_PLAIN || a.est == EST_COUPLED))
         packed = lookup_sobol_packed(k.model, a.p->kind, a.est == EST_COUPLED);
     if (packed) fn = packed;
-    // few, long raw-ordered paths (fewer 32-path groups than 8 warps per SM): helper warps
-    // generate each path-owning warp's normals
+    // few, long raw-ordered paths (fewer 32-path groups than 8 warps per SM, at least 256 normals
+    // a path): helper warps generate each path-owning warp's normals.  Measured on 512 groups:
+    // 1.1-2x faster from 256 normals up, slower below 128 (the ring's handoffs cost more than
+    // the generation they hide)
     const void* assist = nullptr;
-    if (!a.dump && !packed && a.noise == NOISE_RAW && D >= 64 && (a.est == EST_PLAIN || a.est == EST_COUPLED)) {
+    if (!a.dump && !packed && a.noise == NOISE_RAW && D >= 256 && (a.est == EST_PLAIN || a.est == EST_COUPLED)) {
         const uint64_t groups = (((a.offset + a.n_points - 1) >> 5) - (a.offset >> 5) + 1) * (uint64_t)a.R;
         if (groups < (uint64_t)E.sm_count * 8)
             assist = lookup_assist(a.gen, k.model, a.p->kind, a.est == EST_COUPLED);

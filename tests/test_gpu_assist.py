@@ -1,6 +1,6 @@
 """Assisted passes: raw-ordered passes with few 32-path groups and long paths, where three helper
 warps generate each path-owning warp's normals.  On one B200 (148 SMs) a pass is assisted when it
-has fewer than 148 x 8 groups.  The same points priced as replica 0 of a one-replica pass
+has fewer than 148 x 8 groups and at least 256 normals per path.  The same points priced as replica 0 of a one-replica pass
 (assisted, 800 groups) and of a two-replica pass (1600 groups, the plain loop) have the same work
 items, so their sums must agree bit for bit; the oracle checks the values."""
 import numpy as np
@@ -30,7 +30,7 @@ def _payoff(gpu, name):
             "downout": lambda: gpu.barrier_down_out(100.0, 85.0, 0.2, 0.05, 1.0)}[name]()
 
 
-@pytest.mark.parametrize("model,steps", [("gbm", 96), ("heston", 64), ("dupire", 100), ("lv", 64)])
+@pytest.mark.parametrize("model,steps", [("gbm", 300), ("heston", 128), ("dupire", 260), ("lv", 256)])
 @pytest.mark.parametrize("pay", ["asian", "lookback"])
 def test_assisted_pass_equals_plain_loop(gpu, model, steps, pay):
     m, p = _model(gpu, model), _payoff(gpu, pay)
@@ -49,7 +49,7 @@ def test_assisted_coupled_level_equals_plain_loop(gpu, model, use_sobol):
     assert np.array_equal(one[0], two[0]), (one, two)
 
 
-@pytest.mark.parametrize("model,steps", [("gbm", 64), ("heston", 40), ("dupire", 70), ("lv", 96)])
+@pytest.mark.parametrize("model,steps", [("gbm", 256), ("heston", 130), ("dupire", 270), ("lv", 288)])
 @pytest.mark.parametrize("pay", ["eur", "asian", "downout"])
 def test_assisted_pass_vs_oracle(gpu, orc, model, steps, pay):
     m, p = _model(gpu, model), _payoff(gpu, pay)
