@@ -1,8 +1,9 @@
 """Assisted passes: raw-ordered passes with few 32-path groups and long paths, where three helper
 warps generate each path-owning warp's normals.  On one B200 (148 SMs) a pass is assisted when it
-has fewer than 148 x 8 groups and at least 256 normals per path.  The same points priced as replica 0 of a one-replica pass
-(assisted, 800 groups) and of a two-replica pass (1600 groups, the plain loop) have the same work
-items, so their sums must agree bit for bit; the oracle checks the values."""
+has fewer than 148 x 8 groups and at least 256 normals per path.  The same points priced as
+replica 0 of a one-replica pass (assisted, 800 groups) and of a two-replica pass (1600 groups, the
+plain loop) have the same work items, so their sums must agree bit for bit; the oracle checks the
+values."""
 import numpy as np
 import pytest
 
