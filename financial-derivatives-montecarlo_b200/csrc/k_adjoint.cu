@@ -112,19 +112,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             for (int d0 = 0; d0 < N; d0 += 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
-                // the step loops read this lane's row of the tile from shared memory and stay
-                // mostly rolled: fully unrolled, the sweeps overflowed the instruction cache
-#pragma unroll 4
-                for (int i = 0; i < 32; i++) {
-                    const int k = d0 + i;
-                    if ((i & (kCk - 1)) == 0) ck[(k / kCk) * 32 + lane] = S;
-                    float dsS, dsP;
-                    LvEval lv;
-                    const float sig = local_sigma<MOD>(p, S, (float)k * h, &dsS, &dsP, &lv);
-                    S = fmaf(S, fmaf(sig, buf[swz(lane, i)] * sqh, muh), S);
-                    if constexpr (PAY == PAY_ASIAN) ts += S;
-                    if constexpr (PAY == PAY_LOOKBACK) {
-                        if (S < mn) { mn = S; kmin = k + 1; }
+                // the step loops read this lane's row of the tile from shared memory, four steps
+                // per float4 (the swizzled layout makes row reads conflict-free), and stay rolled
+                // over the chunks: fully unrolled, the sweeps overflowed the instruction cache
+                const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
+#pragma unroll 1
+                for (int c = 0; c < 8; c++) {
+                    const float4 v4 = row4[c ^ (lane & 7)];
+                    const float zc[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int i = 4 * c + q;
+                        const int k = d0 + i;
+                        if ((i & (kCk - 1)) == 0) ck[(k / kCk) * 32 + lane] = S;
+                        float dsS, dsP;
+                        LvEval lv;
+                        const float sig = local_sigma<MOD>(p, S, (float)k * h, &dsS, &dsP, &lv);
+                        S = fmaf(S, fmaf(sig, zc[q] * sqh, muh), S);
+                        if constexpr (PAY == PAY_ASIAN) ts += S;
+                        if constexpr (PAY == PAY_LOOKBACK) {
+                            if (S < mn) { mn = S; kmin = k + 1; }
+                        }
                     }
                 }
                 if constexpr (PAY == PAY_ASIAN) { kadd(tot, comp, ts); ts = 0.f; }
@@ -149,45 +157,58 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
+                const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
 #pragma unroll 1
                 for (int s = 1; s >= 0; s--) {
                     const int k0 = d0 + s * kCk;
                     float Sr = ck[(k0 / kCk) * 32 + lane];
-#pragma unroll 4
-                    for (int i = 0; i < kCk; i++) {
-                        seg[i * 32 + lane] = Sr;
-                        float dsS, dsP;
-                        LvEval lv;
-                        const float sig = local_sigma<MOD>(p, Sr, (float)(k0 + i) * h, &dsS, &dsP, &lv);
-                        Sr = fmaf(Sr, fmaf(sig, buf[swz(lane, s * kCk + i)] * sqh, muh), Sr);
-                    }
-#pragma unroll 4
-                    for (int i = kCk - 1; i >= 0; i--) {
-                        const int k = k0 + i;
-                        const float Sk = seg[i * 32 + lane];
-                        const float dw = buf[swz(lane, s * kCk + i)] * sqh;
-                        float dsS, dsP;
-                        LvEval lv;
-                        const float sig = local_sigma<MOD>(p, Sk, (float)k * h, &dsS, &dsP, &lv);
-                        mubar = fmaf(Sbar, Sk * h, mubar);
-                        const float sens = Sbar * Sk * dw;     // dP/dsigma_k through this step
-                        sigbar = fmaf(sens, dsP, sigbar);
-                        // the parametric Dupire volatility is scaled by the model's S0 itself:
-                        // d sigma_k / d S0 = -(beta - 1) sigma_k / S0 enters the delta
-                        if constexpr (MOD == MOD_DUPIRE) s0bar = fmaf(sens, -p.bm1 * sig * p.inv_S0, s0bar);
-                        if constexpr (MOD == MOD_LVGRID) {
-                            if (valid && sens != 0.f) {
-                                atomicAdd(&nodes[lv.n00], (double)(sens * lv.w00));
-                                atomicAdd(&nodes[lv.n00 + 1], (double)(sens * lv.w01));
-                                atomicAdd(&nodes[lv.n00 + p.lv_nK], (double)(sens * lv.w10));
-                                atomicAdd(&nodes[lv.n00 + p.lv_nK + 1], (double)(sens * lv.w11));
-                            }
+#pragma unroll 1
+                    for (int c = 0; c < kCk / 4; c++) {
+                        const float4 v4 = row4[(s * (kCk / 4) + c) ^ (lane & 7)];
+                        const float zc[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const int i = 4 * c + q;
+                            seg[i * 32 + lane] = Sr;
+                            float dsS, dsP;
+                            LvEval lv;
+                            const float sig = local_sigma<MOD>(p, Sr, (float)(k0 + i) * h, &dsS, &dsP, &lv);
+                            Sr = fmaf(Sr, fmaf(sig, zc[q] * sqh, muh), Sr);
                         }
-                        const float dS1 = 1.f + muh + sig * dw + Sk * dw * dsS;
-                        float direct = 0.f;
-                        if constexpr (PAY == PAY_ASIAN) direct = (k >= 1) ? g_all : 0.f;
-                        if constexpr (PAY == PAY_LOOKBACK) direct = (k == kmin) ? -p.corr_f : 0.f;
-                        Sbar = fmaf(Sbar, dS1, direct);
+                    }
+#pragma unroll 1
+                    for (int c = kCk / 4 - 1; c >= 0; c--) {
+                        const float4 v4 = row4[(s * (kCk / 4) + c) ^ (lane & 7)];
+                        const float zc[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int q = 3; q >= 0; q--) {
+                            const int i = 4 * c + q;
+                            const int k = k0 + i;
+                            const float Sk = seg[i * 32 + lane];
+                            const float dw = zc[q] * sqh;
+                            float dsS, dsP;
+                            LvEval lv;
+                            const float sig = local_sigma<MOD>(p, Sk, (float)k * h, &dsS, &dsP, &lv);
+                            mubar = fmaf(Sbar, Sk * h, mubar);
+                            const float sens = Sbar * Sk * dw;     // dP/dsigma_k through this step
+                            sigbar = fmaf(sens, dsP, sigbar);
+                            // the parametric Dupire volatility is scaled by the model's S0 itself:
+                            // d sigma_k / d S0 = -(beta - 1) sigma_k / S0 enters the delta
+                            if constexpr (MOD == MOD_DUPIRE) s0bar = fmaf(sens, -p.bm1 * sig * p.inv_S0, s0bar);
+                            if constexpr (MOD == MOD_LVGRID) {
+                                if (valid && sens != 0.f) {
+                                    atomicAdd(&nodes[lv.n00], (double)(sens * lv.w00));
+                                    atomicAdd(&nodes[lv.n00 + 1], (double)(sens * lv.w01));
+                                    atomicAdd(&nodes[lv.n00 + p.lv_nK], (double)(sens * lv.w10));
+                                    atomicAdd(&nodes[lv.n00 + p.lv_nK + 1], (double)(sens * lv.w11));
+                                }
+                            }
+                            const float dS1 = 1.f + muh + sig * dw + Sk * dw * dsS;
+                            float direct = 0.f;
+                            if constexpr (PAY == PAY_ASIAN) direct = (k >= 1) ? g_all : 0.f;
+                            if constexpr (PAY == PAY_LOOKBACK) direct = (k == kmin) ? -p.corr_f : 0.f;
+                            Sbar = fmaf(Sbar, dS1, direct);
+                        }
                     }
                 }
                 __syncwarp();
