@@ -9,7 +9,8 @@
 //     Sbar_k = Sbar_{k+1} dS_{k+1}/dS_k + dP/dS_k,
 //     mubar += Sbar_{k+1} S_k h,            sigmabar += Sbar_{k+1} dS_{k+1}/dsigma,
 // and, for the grid local-vol model, adds Sbar_{k+1} S_k dW_k w_n to the four bilinear nodes n of
-// (S_k, t_k) in an FP64 shared-memory array per CTA.  Payoffs are the Lipschitz ones:
+// (S_k, t_k) in an FP64 shared-memory array per CTA (summed per lane over the consecutive steps
+// that stay in one grid cell, then added with one atomic per node).  Payoffs are the Lipschitz ones:
 // European (discounted), arithmetic Asian and floating-strike lookback (BGK factor constant).
 // Per path it yields P, delta = Sbar_0 (plus, for the parametric Dupire model, whose volatility
 // (S/S0)^(beta-1) is scaled by S0, the sensitivity through that scale, so that delta is the
@@ -154,6 +155,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             }
             // ---------------- reverse sweep
             float mubar = 0.f, sigbar = 0.f, s0bar = 0.f;
+            // grid local vol: the node sensitivities of consecutive steps in the same cell are
+            // summed in registers (FP64) and added to the CTA's node array when the cell changes
+            int vcell = -1;
+            double v00 = 0.0, v01 = 0.0, v10 = 0.0, v11 = 0.0;
             for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
@@ -197,10 +202,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                             if constexpr (MOD == MOD_DUPIRE) s0bar = fmaf(sens, -p.bm1 * sig * p.inv_S0, s0bar);
                             if constexpr (MOD == MOD_LVGRID) {
                                 if (valid && sens != 0.f) {
-                                    atomicAdd(&nodes[lv.n00], (double)(sens * lv.w00));
-                                    atomicAdd(&nodes[lv.n00 + 1], (double)(sens * lv.w01));
-                                    atomicAdd(&nodes[lv.n00 + p.lv_nK], (double)(sens * lv.w10));
-                                    atomicAdd(&nodes[lv.n00 + p.lv_nK + 1], (double)(sens * lv.w11));
+                                    if (lv.n00 != vcell) {
+                                        if (vcell >= 0) {
+                                            atomicAdd(&nodes[vcell], v00);
+                                            atomicAdd(&nodes[vcell + 1], v01);
+                                            atomicAdd(&nodes[vcell + p.lv_nK], v10);
+                                            atomicAdd(&nodes[vcell + p.lv_nK + 1], v11);
+                                        }
+                                        vcell = lv.n00;
+                                        v00 = v01 = v10 = v11 = 0.0;
+                                    }
+                                    v00 += (double)(sens * lv.w00);
+                                    v01 += (double)(sens * lv.w01);
+                                    v10 += (double)(sens * lv.w10);
+                                    v11 += (double)(sens * lv.w11);
                                 }
                             }
                             const float dS1 = 1.f + muh + sig * dw + Sk * dw * dsS;
@@ -212,6 +227,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                     }
                 }
                 __syncwarp();
+            }
+            if constexpr (MOD == MOD_LVGRID) {
+                if (vcell >= 0) {
+                    atomicAdd(&nodes[vcell], v00);
+                    atomicAdd(&nodes[vcell + 1], v01);
+                    atomicAdd(&nodes[vcell + p.lv_nK], v10);
+                    atomicAdd(&nodes[vcell + p.lv_nK + 1], v11);
+                }
             }
             float rho = mubar;
             if constexpr (PAY == PAY_EUR) rho -= p.pay_T * P;
