@@ -79,6 +79,13 @@ __host__ __device__ inline int book_class(int d) { return (d - 1) >> 2; }
 constexpr int kBookLsFloats = kMaxBasket * kMaxBasket;
 constexpr int kBookAssetFloats = 4 * kMaxBasket;   // sigma, S0, weight, weight / S0 per asset
 constexpr int kBookWarpFloats = 1024 + kBookLsFloats + kBookAssetFloats + 2 * kBookNST;
+// Baskets of 11 and 12 assets leave many lanes of a step-major tile idle (a 32-dimension tile holds
+// 22 or 24 whole-step dimensions); they generate two tiles at a time instead, holding 64 / d whole
+// steps (55 or 60 of 64 lanes busy): 1.08-1.17x on their slices.  Their class (d 9-12) gets a second
+// transpose tile after the per-warp area.  Pairing gained nothing at d = 9 and cost 4-7 % in the
+// d 5-8 class (d = 7, and d = 8 through the larger kernel), so those keep single tiles.
+__host__ __device__ constexpr bool book_pair_tiles(int d) { return d == 11 || d == 12; }
+__host__ __device__ constexpr int book_warp_floats(int cls) { return kBookWarpFloats + (cls == 2 ? 1024 : 0); }
 
 // A float4 of shared memory, read at every use.  The Cholesky rows are loop-invariant and the
 // compiler otherwise keeps the factor in registers across the chunk; for baskets of up to four
@@ -284,6 +291,42 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
             }
             __syncwarp();
         }
+    } else if constexpr (book_pair_tiles(D)) {
+        // two tiles per round: dimensions k0 D .. k0 D + 63, S2 = 64 / D whole steps
+        constexpr int S2 = 64 / D, W2 = S2 * D;
+        float* buf2 = buf + kBookWarpFloats;
+        for (uint64_t g = gb; g < ge; g++) {
+            P path;
+            path.init(sg);
+            for (int k0 = 0; k0 < nf; k0 += S2) {
+                const int dim = k0 * D + lane;
+                sobol_tile(dr, dstride, dim, dim < Dt, g, a.u_cap, buf, lane);
+                sobol_tile(dr, dstride, dim + 32, lane < W2 - 32 && dim + 32 < Dt, g, a.u_cap, buf2, lane);
+                __syncwarp();
+                const float4* rowA = reinterpret_cast<const float4*>(buf + lane * 32);
+                const float4* rowB = reinterpret_cast<const float4*>(buf2 + lane * 32);
+#pragma unroll
+                for (int st = 0; st < S2; st++) {
+                    if (k0 + st < nf) {
+                        float x[D];
+#pragma unroll
+                        for (int c = 0; c < D; c++) {
+                            const int col = st * D + c;
+                            const float4 v = (col < 32) ? rowA[(col >> 2) ^ (lane & 7)]
+                                                        : rowB[((col - 32) >> 2) ^ (lane & 7)];
+                            const float zc = (col & 3) == 0 ? v.x : (col & 3) == 1 ? v.y : (col & 3) == 2 ? v.z : v.w;
+                            x[c] = zc * sqrt_h;
+                        }
+                        path.step(x, L4, sg, muh_f, muh_c, Mc);
+                    }
+                }
+                __syncwarp();
+            }
+            float y[NS];
+            path.finish(sg, K, disc, has_c, y);
+            const uint64_t n = g * 32 + (uint64_t)lane;
+            acc.add(y, n >= s.offset && n < pend, lane);
+        }
     } else {
         for (uint64_t g = gb; g < ge; g++) {
             P path;
@@ -326,7 +369,7 @@ template <int CLS, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__ BookArgs a) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    float* buf = reinterpret_cast<float*>(smem4) + wib * kBookWarpFloats;
+    float* buf = reinterpret_cast<float*>(smem4) + wib * book_warp_floats(CLS);
     float* Ls = buf + 1024;
     double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats + kBookAssetFloats);
     const int c_end = a.hdr[3 + CLS];
@@ -439,7 +482,7 @@ namespace {
 
 constexpr int kIterCap = 50;   // run_mlqmc_cuda's iteration cap (:1950)
 
-size_t book_smem() { return (size_t)kWarpsPerBlock * kBookWarpFloats * sizeof(float); }
+size_t book_smem(int cls) { return (size_t)kWarpsPerBlock * book_warp_floats(cls) * sizeof(float); }
 
 // Resident CTAs per SM each width class is compiled for (its register budget).
 using BookFn = void (*)(BookArgs);
@@ -702,9 +745,9 @@ struct BookRunner {
         static int per_sm[kBookClasses] = {-1, -1, -1, -1};
         if (per_sm[cls] < 0) {
             const void* fn = (const void*)book_fn(cls);
-            MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)book_smem()));
+            MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)book_smem(cls)));
             int b = 0;
-            MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, book_smem()));
+            MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, book_smem(cls)));
             MCQ_REQUIRE(b > 0, MCQ_ERR_INTERNAL, "book kernel does not fit on an SM");
             per_sm[cls] = b;
         }
@@ -713,7 +756,7 @@ struct BookRunner {
 
     void launch_book(int cls, const BookArgs& a, int grid, cudaStream_t st_) {
         void* argv[] = {(void*)&a};
-        MCQ_CUDA(cudaLaunchKernel((const void*)book_fn(cls), dim3(grid), dim3(kThreads), argv, book_smem(), st_));
+        MCQ_CUDA(cudaLaunchKernel((const void*)book_fn(cls), dim3(grid), dim3(kThreads), argv, book_smem(cls), st_));
     }
     void launch_fin(const BookArgs& a, int grid, cudaStream_t st_) {
         void* argv[] = {(void*)&a};

@@ -28,7 +28,9 @@ def _basket(eng, d, seed, eps=2e-3, max_L=5, T=1.0, r=0.03, corr=True, kmul=1.0)
 
 
 @pytest.mark.parametrize("d,level,corr", [(1, 0, True), (3, 1, True), (4, 3, False), (7, 2, True),
-                                          (12, 1, True), (16, 4, True)])
+                                          (12, 1, True), (16, 4, True),
+                                          # long step-major paths; paired tiles at d = 11, 12
+                                          (7, 5, True), (9, 4, True), (11, 3, False), (12, 5, True)])
 def test_book_slice_sums_match_oracle(gpu, orc, d, level, corr):
     """Per-replica sums of one slice (ragged offset and count) through the book kernel against
     the FP64 oracle of the coupled basket pair with pathwise deltas."""
