@@ -137,6 +137,21 @@ int mcq_bb_create(int N, double T, mcq_handle* out) {
         H->host_f[3 * j + 2] = (float)sd[j];
         H->host_i[j] = map[j];
     }
+    if (N > 32) {   // window levels of the fused bridge (bb_window): are their weights uniform?
+        const int S = N >> 5;
+        bool uni = true;
+        for (int u = 0; u < 5 && uni; u++) {
+            const int d0 = S << u;
+            for (int c = 0; c < 3; c++) H->bb_lvl[u][c] = H->host_f[3 * d0 + c];
+            for (int q = 0; q < S && uni; q++)
+                for (int v = 0; v < (1 << u) && uni; v++) {
+                    const int d = (S << u) + (q << u) + v;
+                    for (int c = 0; c < 3; c++)
+                        if (std::memcmp(&H->host_f[3 * d + c], &H->bb_lvl[u][c], sizeof(float)) != 0) uni = false;
+                }
+        }
+        H->bb_uni = uni;
+    }
     try {
         char* d = (char*)H->table.ensure(sizeof(float4) * N + sizeof(int2) * N);
         MCQ_CUDA(cudaMemcpy(d, w4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));

@@ -15,6 +15,7 @@ const void* lookup_sobol_packed(int model, int payoff, bool coupled);   // raw, 
 const void* lookup_assist(int gen, int model, int payoff, bool coupled);  // raw, few long paths (NOISE_ASSIST)
 const void* lookup_sobol_bb(int model, int payoff, bool coupled);
 const void* lookup_sobol_bb_b3(int model, int payoff);          // 3-CTA (80-register) variant
+const void* lookup_sobol_bbu(int model, int payoff, bool coupled, int variant);   // NOISE_BB_UNI
 const void* lookup_sobol_pca_small(int model, int payoff, bool coupled);   // N <= 32
 const void* lookup_philox_plain(int model, int payoff);
 const void* lookup_philox_coupled(int model, int payoff);
@@ -28,11 +29,13 @@ inline int n_variants(int gen, int noise, int est, int model) {
     if (est != EST_PLAIN) return 1;
     if (noise == NOISE_RAW) return 3;
     if (noise == NOISE_BB && model != MOD_HESTON) return 2;
+    if (noise == NOISE_BB_UNI && model != MOD_HESTON) return 3;
     return 1;
 }
 inline const void* lookup_variant(int gen, int noise, int est, int model, int payoff, int variant) {
     if (variant < 1 || variant >= n_variants(gen, noise, est, model)) return nullptr;
     if (est == EST_COUPLED) return lookup_sobol_raw_coupled_b4(model, payoff);
+    if (noise == NOISE_BB_UNI) return lookup_sobol_bbu(model, payoff, false, variant);
     if (noise == NOISE_RAW) return variant == 1 ? lookup_sobol_raw_plain_b4(model, payoff) : lookup_sobol_raw_plain_b5(model, payoff);
     return lookup_sobol_bb_b3(model, payoff);
 }
@@ -44,6 +47,7 @@ inline const void* lookup_pass(int gen, int noise, int est, int model, int payof
     if (gen == GEN_SOBOL) {
         if (noise == NOISE_RAW) return cpl ? lookup_sobol_raw_coupled(model, payoff) : lookup_sobol_raw_plain(model, payoff);
         if (noise == NOISE_BB) return lookup_sobol_bb(model, payoff, cpl);
+        if (noise == NOISE_BB_UNI) return lookup_sobol_bbu(model, payoff, cpl, 0);
         if (noise == NOISE_PCA) return lookup_sobol_pca_small(model, payoff, cpl);
         return nullptr;
     }

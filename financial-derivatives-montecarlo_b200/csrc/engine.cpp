@@ -341,7 +341,10 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
         MCQ_REQUIRE(a.gen == GEN_SOBOL, MCQ_ERR_UNSUPPORTED, "Brownian bridge is a QMC transform");
         k.bb = (const float4*)a.bb->table.p;
         k.bbi = (const int2*)((const float4*)a.bb->table.p + a.n_steps);
+        if (a.bb->bb_uni) std::memcpy(k.bbw, a.bb->bb_lvl, sizeof(k.bbw));
     }
+    // the kernel family: the bridge with uniform window weights reads them from the parameters
+    const int knoise = (a.noise == NOISE_BB && D > 32 && a.bb->bb_uni) ? NOISE_BB_UNI : a.noise;
     const bool pca_tc = (a.noise == NOISE_PCA) && D >= 64;
     if (a.noise == NOISE_PCA) {
         MCQ_REQUIRE(k.d_noise == 1, MCQ_ERR_UNSUPPORTED, "PCA needs a one-factor model");
@@ -358,7 +361,7 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     }
 
     const void* fn = a.dump ? lookup_misc(a.gen, a.noise, a.est, k.model, nb, true)
-                            : lookup_pass(a.gen, a.noise, a.est, k.model, a.p->kind, nb);
+                            : lookup_pass(a.gen, knoise, a.est, k.model, a.p->kind, nb);
     // short raw-ordered Sobol paths: 32 / D path groups per tile instead of one
     const void* packed = nullptr;
     if (!a.dump && a.gen == GEN_SOBOL && a.noise == NOISE_RAW && D <= 16 &&
@@ -379,13 +382,13 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     // launch variant: MCQ_TUNE=<v> forces one; otherwise the autotuner picks per family
     int variant = 0;
     TuneState* trial = nullptr;
-    const int nvar = (a.dump || packed || assist) ? 1 : n_variants(a.gen, a.noise, a.est, k.model);
+    const int nvar = (a.dump || packed || assist) ? 1 : n_variants(a.gen, knoise, a.est, k.model);
     if (nvar > 1) {
         const char* force = std::getenv("MCQ_TUNE");
         if (force) {
             variant = std::min(std::max(std::atoi(force), 0), nvar - 1);
         } else {
-            const uint64_t key = (uint64_t)a.gen | ((uint64_t)a.noise << 4) | ((uint64_t)a.est << 8) |
+            const uint64_t key = (uint64_t)a.gen | ((uint64_t)knoise << 4) | ((uint64_t)a.est << 8) |
                                  ((uint64_t)k.model << 12) | ((uint64_t)a.p->kind << 16);
             TuneState& ts = E.tune[key];
             for (int v = 0; v < nvar; v++) {
@@ -423,7 +426,7 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
                 }
             }
         }
-        if (variant > 0) fn = lookup_variant(a.gen, a.noise, a.est, k.model, a.p->kind, variant);
+        if (variant > 0) fn = lookup_variant(a.gen, knoise, a.est, k.model, a.p->kind, variant);
     }
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED,
                 "no fused kernel for gen " + std::to_string(a.gen) + " noise " + std::to_string(a.noise) +

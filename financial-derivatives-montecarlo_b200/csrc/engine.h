@@ -71,6 +71,10 @@ struct Handle {
     DevBuf table;       // BB: float4[N] + int2[N]; PCA: fp16 [m][m] row-major (row = output step)
     std::vector<float> host_f;   // BB: wl,wr,sd per dim; PCA: column-major float M
     std::vector<int> host_i;     // BB: m per dim
+    // BB, N > 32: true when every window point of a level has the same (wl, wr, sd) in FP32 (a
+    // uniform time grid); bb_lvl[u] is that triple for window level u = 0..4
+    bool bb_uni = false;
+    float bb_lvl[5][3] = {};
 };
 
 struct KernelInfo {

@@ -17,7 +17,9 @@ enum Gen : int { GEN_SOBOL = 0, GEN_PHILOX = 1 };
 // (an engine-internal choice, never requested through the API)
 // NOISE_ASSIST: raw ordering for passes with few, long paths: each path-owning warp is fed its
 // normal tiles by three helper warps (engine-internal as well)
-enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3, NOISE_ASSIST = 4 };
+// NOISE_BB_UNI: the Brownian bridge whose window weights are the same for every point of a level
+// (read from KParams::bbw instead of the per-dimension table; engine-internal)
+enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3, NOISE_ASSIST = 4, NOISE_BB_UNI = 5 };
 
 // Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
 constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
@@ -81,6 +83,7 @@ struct KParams {
     //      bb[j] = {wl, wr, sd, bits(m)}, bbi[j] = {l, r}
     const float4* bb;
     const int2* bbi;
+    float bbw[5][3];    // NOISE_BB_UNI: (wl, wr, sd) of window level u = 0..4
     // ---- PCA: M_pca (fp16, K-major rows = output step) device pointer
     const void* pca;
     // ---- Sobol: pre-scrambled words, replica r at dirs + r * 33 * dstride, word k of dim d at

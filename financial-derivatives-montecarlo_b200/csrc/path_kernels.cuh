@@ -738,7 +738,7 @@ struct BasketWideC {
 // slot s (level u = floor(log2(s+1)), position v = s + 1 - 2^u); its Sobol dimension is
 // (S << u) + (q << u) + v (bb_precompute's level order, utils.cpp:78-99) and its weights are
 // read from the per-dimension table.
-template <class C>
+template <bool UNI, class C>
 __device__ __forceinline__ void bb_window(const KParams& p, C& cons, const float (&zs)[32],
                                           float WL, float WR, int S, int q) {
     float W[33];
@@ -751,8 +751,12 @@ __device__ __forceinline__ void bb_window(const KParams& p, C& cons, const float
             const int s = (1 << u) - 1 + v;
             const int half = 16 >> u;
             const int mid = (2 * v + 1) * half, lft = 2 * v * half, rgt = (2 * v + 2) * half;
-            const int dim = (S << u) + (q << u) + v;
-            const float4 w = __ldg(p.bb + dim);
+            float4 w;
+            if constexpr (UNI) {   // level weights from the parameter block: no loads
+                w = make_float4(p.bbw[u][0], p.bbw[u][1], p.bbw[u][2], 0.f);
+            } else {
+                w = __ldg(p.bb + (S << u) + (q << u) + v);
+            }
             W[mid] = fmaf(w.x, W[lft], fmaf(w.y, W[rgt], w.z * zs[s]));
         }
     }
@@ -862,7 +866,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
                 float z[32];
                 read_row(buf, lane, z);
                 __syncwarp();
-                bb_window(p, cons, z, skel[q * 32 + lane], skel[(q + 1) * 32 + lane], S, q);
+                bb_window<NOISE == NOISE_BB_UNI>(p, cons, z, skel[q * 32 + lane], skel[(q + 1) * 32 + lane], S, q);
             }
         }
     }
@@ -976,6 +980,8 @@ __device__ __forceinline__ void assisted_pass(const KParams& p, unsigned char* s
     if (stop && lane == 0) atomicExch(p.err, MCQ_ERR_TIMEOUT_CODE);
 }
 
+__host__ __device__ constexpr bool noise_is_bb(int noise) { return noise == NOISE_BB || noise == NOISE_BB_UNI; }
+
 // MINB: resident CTAs per SM the register budget is set for (0: 2 for the bridge, whose
 // window keeps 33 W values live, kMinBlocks otherwise).  Variants differ only in register
 // allocation and scheduling, never in arithmetic, so they produce identical sums.
@@ -985,7 +991,7 @@ template <int NB>
 struct warp_acc_of<BasketLevelC<NB>> { static constexpr bool value = true; };
 
 template <int GEN, int NOISE, class C, int MINB = 0>
-__global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ? 2 : kMinBlocks))
+__global__ void __launch_bounds__(kThreads, MINB ? MINB : (noise_is_bb(NOISE) ? 2 : kMinBlocks))
     k_pass(const __grid_constant__ KParams p) {
     extern __shared__ float4 smem4[];
     if constexpr (NOISE == NOISE_ASSIST) {
@@ -994,7 +1000,7 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : ((NOISE == NOISE_BB) ?
     }
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     constexpr bool WACC = warp_acc_of<C>::value;
-    const int skel_floats = (NOISE == NOISE_BB && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;
+    const int skel_floats = (noise_is_bb(NOISE) && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;
     const int acc_floats = WACC ? ((2 * C::NST + 3) & ~3) : 0;
     float* buf = reinterpret_cast<float*>(smem4) + wib * (1024 + skel_floats + acc_floats);
     float* skel = buf + 1024;

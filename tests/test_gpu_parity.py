@@ -184,13 +184,13 @@ def test_bridge_launch_variants_are_bit_identical(gpu, model, pay):
     bb = gpu.bb_create(256, m.T)
     out = []
     try:
-        for v in ("0", "1"):
+        for v in ("0", "1", "2"):   # a uniform time grid: the window weights come from the parameters
             os.environ["MCQ_TUNE"] = v
             out.append(gpu.qmc_pass(m, p, 256, noise=gpu.BB, bb=bb, salt_base=42, R=4, offset=3, n_points=20000))
     finally:
         os.environ.pop("MCQ_TUNE", None)
         bb.close()
-    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
 @pytest.mark.parametrize("pay", ["eur", "lookback", "downout"])
