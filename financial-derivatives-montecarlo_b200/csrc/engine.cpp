@@ -603,7 +603,7 @@ void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t 
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no adjoint kernel for this model / payoff");
     const uint64_t g0 = offset >> 5;
     const uint64_t G = ((offset + n_points - 1) >> 5) - g0 + 1;
-    const long long target = kTargetItems / 2;
+    const long long target = kTargetItemsAdjoint;
     uint64_t gpi = (G * (uint64_t)R + target - 1) / target;
     if (gpi < 1) gpi = 1;
     const uint64_t ipr = (G + gpi - 1) / gpi;

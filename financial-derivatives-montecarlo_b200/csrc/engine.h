@@ -138,8 +138,12 @@ struct PassArgs {
 };
 
 // Work items per pass are sized from the problem alone (never from the device) so that the
-// split, and with it every sum, is the same on any GPU.
-inline constexpr long long kTargetItems = 148LL * 16 * 6;
+// split, and with it every sum, is the same on any GPU.  About eight items per resident warp of a
+// B200 at four CTAs per SM: a warp's last item then costs at most an eighth of the pass (with
+// three per warp the small first passes of the adaptive drivers lost up to a quarter).
+inline constexpr long long kTargetItems = 148LL * 32 * 8;
+// the adjoint's split (two CTAs per SM, checkpoint state per warp)
+inline constexpr long long kTargetItemsAdjoint = 148LL * 16 * 3;
 
 int noise_dim(const mcq_model& m);
 // KParams for a pass (make_params); basket / local-vol arrays are uploaded into ws.aux.
