@@ -374,6 +374,22 @@ struct PathC {
         }
         flush();
     }
+    // Heston: the same steps fed straight from this lane's row of a transposed tile in shared
+    // memory, four normals (two steps) per float4 and the chunk loop rolled; the fully unrolled
+    // sixteen steps of tile() (fine and coarse legs) weighed on the instruction cache
+    static constexpr bool SMEM_TILE = HES;
+    __device__ __forceinline__ void tile_smem(const KParams& p, const float* buf, int lane, int nv) {
+        const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
+#pragma unroll 2
+        for (int c = 0; c < 8; c++) {
+            if (4 * c < nv) {
+                const float4 v = row4[c ^ (lane & 7)];
+                step_dw(p, v.x * p.sqrt_h, fmaf(p.L10, v.x, p.L11 * v.y) * p.sqrt_h);
+                if (4 * c + 2 < nv) step_dw(p, v.z * p.sqrt_h, fmaf(p.L10, v.z, p.L11 * v.w) * p.sqrt_h);
+            }
+        }
+        flush();
+    }
     // fold the running partial sums (called at least every 32 steps)
     __device__ __forceinline__ void flush() {
         f.flush();
@@ -767,6 +783,11 @@ __device__ __forceinline__ void bb_window(const KParams& p, C& cons, const float
 
 // ------------------------------------------------------------------ the pass kernel
 
+template <class C, class = void>
+struct smem_tile_of { static constexpr bool value = false; };
+template <class C>
+struct smem_tile_of<C, std::void_t<decltype(C::SMEM_TILE)>> { static constexpr bool value = C::SMEM_TILE; };
+
 template <int GEN, int NOISE, class C>
 __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint32_t* dr,
                                           uint32_t stream, uint64_t h, uint64_t n, float* buf,
@@ -775,7 +796,13 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
     if constexpr (NOISE == NOISE_RAW) {
         for (int d0 = 0; d0 < D; d0 += 32) {
             float z[32];
-            if constexpr (GEN == GEN_SOBOL) {
+            if constexpr (GEN == GEN_SOBOL && smem_tile_of<C>::value) {
+                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
+                __syncwarp();
+                cons.tile_smem(p, buf, lane, min(32, D - d0));
+                __syncwarp();
+                continue;
+            } else if constexpr (GEN == GEN_SOBOL) {
                 sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
                 __syncwarp();
                 read_row(buf, lane, z);
@@ -938,10 +965,15 @@ __device__ __forceinline__ void assisted_pass(const KParams& p, unsigned char* s
                     const int s = (int)(u % kAssistSlots);
                     const bool ok = asst_wait(&full[s], (u / kAssistSlots) & 1u);
                     if (!__all_sync(0xffffffffu, ok)) { stop = true; break; }
-                    float z[32];
-                    read_row(ring + s * 1024, lane, z);
-                    asst_arrive(&empty[s]);
-                    cons.tile(p, z, min(32, D - 32 * t));
+                    if constexpr (smem_tile_of<C>::value) {
+                        cons.tile_smem(p, ring + s * 1024, lane, min(32, D - 32 * t));
+                        asst_arrive(&empty[s]);
+                    } else {
+                        float z[32];
+                        read_row(ring + s * 1024, lane, z);
+                        asst_arrive(&empty[s]);
+                        cons.tile(p, z, min(32, D - 32 * t));
+                    }
                 }
                 if (stop) break;
                 float y[C::NST];
