@@ -27,7 +27,8 @@ EXPORTS = [
     "mcq_run_mc", "mcq_run_mc_fixed", "mcq_run_qmc", "mcq_run_mlmc", "mcq_run_mlqmc", "mcq_cv_pilot",
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
     "mcq_mc_pass", "mcq_level_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
-    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_qmc_pass_noalloc", "mcq_adjoint",
+    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_debug_wait_timeout", "mcq_qmc_pass_noalloc",
+    "mcq_adjoint",
     "mcq_book_price", "mcq_book_level_sums", "mcq_book_create", "mcq_book_submit", "mcq_book_size",
     "mcq_book_run", "mcq_book_clear", "mcq_book_free",
 ]
@@ -322,6 +323,11 @@ def book_level_sums(option, level, offset=0, n_points=1024, ml=None, qc=None):
     _check(lib().mcq_book_level_sums(C.byref(option), C.byref(ml), C.byref(qc), C.c_int(level), C.c_uint32(offset),
                                      C.c_int64(n_points), out.ctypes.data_as(_P(C.c_double))))
     return out[:, :4 + option.n_assets]
+
+
+def debug_wait_timeout(polls=1000):
+    """mcq_debug_wait_timeout: a bounded device wait that is made to give up (raises MCQError 7)."""
+    _check(lib().mcq_debug_wait_timeout(C.c_uint32(polls)))
 
 
 def mc_pass(m, p, n_steps, seed, stream_id, first_path, n_paths):

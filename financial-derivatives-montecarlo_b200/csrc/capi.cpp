@@ -621,6 +621,21 @@ int mcq_sobol_hh_normal(uint32_t salt, int dim0, int nd, uint32_t offset, int64_
     API_END
 }
 
+int mcq_debug_wait_timeout(uint32_t polls) {
+    API_BEGIN
+    MCQ_REQUIRE(polls >= 1 && polls <= (1u << 20), MCQ_ERR_INVALID, "polls must be 1 .. 2^20");
+    ensure_ready();
+    Workspace& ws = engine().ws(0);
+    int* err = (int*)ws.err.ensure(sizeof(int));
+    MCQ_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ws.stream));
+    ws.err_armed = true;
+    launch_wait_probe(err, polls, ws.stream);
+    MCQ_CUDA(cudaGetLastError());
+    MCQ_CUDA(cudaStreamSynchronize(ws.stream));
+    check_err_word(ws);
+    API_END
+}
+
 int mcq_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     if (!ctr || !key || !out) { g_last_error = "NULL argument"; return MCQ_ERR_INVALID; }
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];

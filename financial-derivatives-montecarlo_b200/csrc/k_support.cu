@@ -89,4 +89,21 @@ void launch_sobol_export(const uint32_t* tab, int D, int dim0, int nd, uint32_t 
     k_sobol_export<<<blocks, 256, 0, s>>>(tab, D, dim0, nd, offset, n, u_cap, as_normal, out);
 }
 
+// Failure-path probe of the bounded mbarrier wait that the assisted passes (and, with the same
+// limit logic, the tensor-core PCA pass) use: one warp waits on a barrier that nothing arrives on,
+// gives up after `polls` polls and records MCQ_ERR_TIMEOUT in the status word, which the host's
+// check turns into the API error.  No fault, no hang: the wait always returns.
+__global__ void k_wait_probe(int* err, uint32_t polls) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asst_addr(&bar)), "r"(1));
+    __syncthreads();
+    const bool ok = asst_wait(&bar, 0u, polls);
+    if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicExch(err, MCQ_ERR_TIMEOUT_CODE);
+}
+
+void launch_wait_probe(int* err, uint32_t polls, cudaStream_t s) {
+    k_wait_probe<<<1, 32, 0, s>>>(err, polls);
+}
+
 }  // namespace mcq

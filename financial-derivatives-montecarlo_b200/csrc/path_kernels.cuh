@@ -914,9 +914,9 @@ __device__ __forceinline__ uint32_t asst_addr(const void* ptr) { return (uint32_
 __device__ __forceinline__ void asst_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(asst_addr(bar)) : "memory");
 }
-__device__ __forceinline__ bool asst_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool asst_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kAssistWaitLimit) {
     const uint32_t a = asst_addr(bar);
-    for (uint32_t i = 0; i < kAssistWaitLimit; i++) {
+    for (uint32_t i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred q;\n mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n"

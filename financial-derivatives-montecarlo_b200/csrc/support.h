@@ -9,6 +9,8 @@ void launch_prescramble(const uint32_t* dv, uint32_t salt0, int R, int D, uint32
                         cudaStream_t s);
 void launch_finalize(const double* partials, int R, int ipr, int nstat, double* out,
                      cudaStream_t s);
+// one warp waits `polls` times on an mbarrier nothing arrives on, then records MCQ_ERR_TIMEOUT
+void launch_wait_probe(int* err, uint32_t polls, cudaStream_t s);
 void launch_sobol_export(const uint32_t* tab, int D, int dim0, int nd, uint32_t offset,
                          long long n, float u_cap, int as_normal, void* out, cudaStream_t s);
 

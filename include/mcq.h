@@ -333,6 +333,10 @@ int mcq_sobol_hh_u32(uint32_t salt, int dim0, int nd, uint32_t offset, int64_t n
                      uint32_t* out_host);
 int mcq_sobol_hh_normal(uint32_t salt, int dim0, int nd, uint32_t offset, int64_t n,
                         int flags, float* out_host);
+/* Failure-path probe: one warp waits `polls` (1 .. 2^20) times on a device barrier that nothing
+   completes, as the bounded waits of the assisted and tensor-core passes do, and returns
+   MCQ_ERR_TIMEOUT through the same status word; the context stays usable. */
+int mcq_debug_wait_timeout(uint32_t polls);
 /* Philox4x32-10 block (counter, key) -> 4 words; host-side, for known-answer checks. */
 int mcq_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* BB / PCA tables as the device sees them (for parity tests). */

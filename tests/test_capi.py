@@ -72,6 +72,8 @@ def test_null_and_bad_arguments_return_status(eng):
     assert L.mcq_sobol_hh_u32(42, 19999, 2, 0, 10, p32) == 4             # dims beyond the table
     assert L.mcq_sobol_hh_u32(42, 0, 1, C.c_uint32(0xFFFFFFF0), C.c_int64(100), p32) == 4  # index beyond 2^32
     assert L.mcq_philox4x32_10(None, None, None) == 1
+    assert L.mcq_debug_wait_timeout(C.c_uint32(0)) == 1                   # polls out of range
+    assert L.mcq_debug_wait_timeout(C.c_uint32(1 << 21)) == 1
 
 
 def test_error_message_is_thread_local(eng):

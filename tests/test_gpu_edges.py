@@ -61,3 +61,16 @@ def test_range_errors(gpu):
     with pytest.raises(gpu.MCQError) as e:
         gpu.qmc_pass(h, p, 10001, salt_base=42, R=1, n_points=32)   # 20002 dimensions
     assert e.value.code == 4
+
+
+def test_bounded_wait_reports_timeout_and_the_context_survives(gpu, orc):
+    """A bounded device wait that nothing completes gives up, the host reads MCQ_ERR_TIMEOUT from
+    the status word, and the next pass runs normally."""
+    with pytest.raises(gpu.MCQError) as e:
+        gpu.debug_wait_timeout(1000)
+    assert e.value.code == 7
+    assert b"timed out" in gpu.lib().mcq_last_error()
+    m, p = gpu.gbm(100.0, 0.05, 0.2, 1.0), gpu.asian(100.0)
+    g = gpu.qmc_pass(m, p, 64, salt_base=42, R=2, offset=3, n_points=2000)
+    o = orc.qmc_sums(m, p, 64, None, salt_base=42, R=2, offset=3, N=2000)
+    assert _close(g, o, 2000), (g, o)
