@@ -74,3 +74,25 @@ def test_bounded_wait_reports_timeout_and_the_context_survives(gpu, orc):
     g = gpu.qmc_pass(m, p, 64, salt_base=42, R=2, offset=3, n_points=2000)
     o = orc.qmc_sums(m, p, 64, None, salt_base=42, R=2, offset=3, N=2000)
     assert _close(g, o, 2000), (g, o)
+
+
+def test_assisted_pass_at_the_last_points_and_many_dimensions(gpu, orc):
+    """An assisted pass (few groups, long paths): Heston with 10000 Sobol dimensions on the last
+    3200 points below 2^32."""
+    m, p = gpu.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0), gpu.lookback(0.2)
+    N = 3200
+    off = (1 << 32) - N
+    g = gpu.qmc_pass(m, p, 5000, salt_base=3, R=1, offset=off, n_points=N)
+    o = orc.qmc_sums(m, p, 5000, None, salt_base=3, R=1, offset=off, N=N)
+    assert _close(g, o, N), (g, o)
+
+
+@pytest.mark.parametrize("R", [1, 32])
+def test_packed_pass_at_the_last_points(gpu, orc, R):
+    """A packed pass (paths of 3 normals, 10 groups per tile) ending at 2^32, with one and 32 replicas."""
+    m, p = gpu.gbm(100.0, 0.05, 0.2, 1.0), gpu.asian(100.0)
+    N = 1000
+    off = (1 << 32) - N
+    g = gpu.qmc_pass(m, p, 3, salt_base=11, R=R, offset=off, n_points=N)
+    o = orc.qmc_sums(m, p, 3, None, salt_base=11, R=R, offset=off, N=N)
+    assert _close(g, o, N), (g, o)
