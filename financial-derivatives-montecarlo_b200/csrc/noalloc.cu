@@ -10,7 +10,7 @@
 //
 // Limits: at most kMaxDims Sobol dimensions (steps x factors), kMaxReplicas replicas and
 // kMaxItems work items; one-factor or Heston models without parameter arrays (GBM, Heston,
-// parametric Dupire), raw noise ordering.  The array costs kScratchBytes (about 2.4 MiB) on
+// parametric Dupire), raw noise ordering.  The array costs kScratchBytes (about 2.7 MiB) on
 // every GPU that loads the library, held until the process exits.
 //
 // Sharing: every call uses the same array and it keeps the last call's contents.  Nothing in
@@ -39,10 +39,13 @@ namespace mcq {
 
 constexpr int kMaxDims = 512;
 constexpr int kMaxReplicas = 32;
-constexpr int kMaxItems = 16384;
+// the work split of kTargetItems yields at most kTargetItems + R items, so every pass the
+// allocating entry point runs (with the same split, hence the same sums) fits
+constexpr int kMaxItems = 38912;
+static_assert(kMaxItems >= kTargetItems + kMaxReplicas, "partials sized for the engine's work split");
 constexpr size_t kTableBytes = (size_t)kMaxDims * 32 * sizeof(uint32_t);              // 64 KiB
 constexpr size_t kDirsBytes = (size_t)kMaxReplicas * 33 * kMaxDims * sizeof(uint32_t); // 2.06 MiB
-constexpr size_t kPartialBytes = (size_t)kMaxItems * 2 * sizeof(double);              // 256 KiB
+constexpr size_t kPartialBytes = (size_t)kMaxItems * 2 * sizeof(double);              // 608 KiB
 constexpr size_t kScratchBytes = kTableBytes + kDirsBytes + kPartialBytes;
 static_assert(kTableBytes % 256 == 0 && kDirsBytes % 256 == 0, "256-byte aligned sections");
 

@@ -314,7 +314,7 @@ int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, i
  * the reference.  For callers that may not call cudaMalloc: code living in a process whose GPU
  * memory belongs to another allocator (a framework's caching allocator, a plugin host with a
  * fixed budget) and latency-critical paths where cudaMalloc / cudaFree would synchronise the
- * device.  Its scratch is one fixed __device__ array inside the library (about 2.4 MiB, held on
+ * device.  Its scratch is one fixed __device__ array inside the library (about 2.7 MiB, held on
  * every GPU that loads the library until exit); sums_device ([R][2] doubles) is the caller's.
  * Limits: GBM, Heston or parametric Dupire, raw ordering, n_steps x factors <= 512, R <= 32;
  * larger requests fail with MCQ_ERR_RANGE.  The first call on a device sets the array up

@@ -29,6 +29,17 @@ def test_noalloc_matches_allocating_pass(eng):
         a, b = out.cpu().numpy().reshape(R, 2), ref.cpu().numpy().reshape(R, 2)
         np.testing.assert_allclose(a, b, rtol=1e-12, atol=0.0, err_msg=f"call {call}")
         assert np.all(a[:, 0] / n > 5) and np.all(a[:, 0] / n < 8)
+    # a large pass (2^20 points x 32 replicas: the work split's full item count) fits the scratch
+    R2 = 32
+    ref2 = torch.zeros(2 * R2, dtype=torch.float64, device="cuda")
+    out2 = torch.zeros(2 * R2, dtype=torch.float64, device="cuda")
+    eng.qmc_pass_noalloc(m, p, n_steps, out2.data_ptr(), stream.cuda_stream, salt_base=42, R=R2, offset=0,
+                         n_points=1 << 20)
+    stream.synchronize()
+    eng.qmc_pass_device(m, p, n_steps, ref2.data_ptr(), stream.cuda_stream, salt_base=42, R=R2, offset=0,
+                        n_points=1 << 20)
+    stream.synchronize()
+    np.testing.assert_allclose(out2.cpu().numpy(), ref2.cpu().numpy(), rtol=1e-12, atol=0.0)
     # a call after set-up takes no device memory
     torch.cuda.synchronize()
     before = torch.cuda.mem_get_info()[0]
