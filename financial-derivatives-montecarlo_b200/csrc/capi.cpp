@@ -626,9 +626,7 @@ int mcq_debug_wait_timeout(uint32_t polls) {
     MCQ_REQUIRE(polls >= 1 && polls <= (1u << 20), MCQ_ERR_INVALID, "polls must be 1 .. 2^20");
     ensure_ready();
     Workspace& ws = engine().ws(0);
-    int* err = (int*)ws.err.ensure(sizeof(int));
-    MCQ_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ws.stream));
-    ws.err_armed = true;
+    int* err = arm_err_word(ws);
     launch_wait_probe(err, polls, ws.stream);
     MCQ_CUDA(cudaGetLastError());
     MCQ_CUDA(cudaStreamSynchronize(ws.stream));

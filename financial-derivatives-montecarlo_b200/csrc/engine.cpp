@@ -480,11 +480,7 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     long long blocks = ((long long)k.n_items + items_per_block - 1) / items_per_block;
     blocks = std::min<long long>(blocks, (long long)ki.blocks_per_sm * E.sm_count);
     blocks = std::max<long long>(blocks, 1);
-    if (assist) {
-        k.err = (int*)ws.err.ensure(sizeof(int));
-        MCQ_CUDA(cudaMemsetAsync(k.err, 0, sizeof(int), ws.stream));
-        ws.err_armed = true;
-    }
+    if (assist) k.err = arm_err_word(ws);
     void* args[] = {&k};
     if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[variant][0], ws.stream));
     MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kThreads), args, smem, ws.stream));
@@ -531,9 +527,7 @@ void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out)
     k.nstat = nst;
     k.partials = (double*)ws.partials.ensure(sizeof(double) * (size_t)k.n_items * pca_warps() * nst);
     if (a.dump) k.dump = (float*)ws.dump.ensure(sizeof(float) * (size_t)a.R * a.n_points * N);
-    k.err = (int*)ws.err.ensure(sizeof(int));
-    MCQ_CUDA(cudaMemsetAsync(k.err, 0, sizeof(int), ws.stream));
-    ws.err_armed = true;
+    k.err = arm_err_word(ws);
     const size_t smem = pca_smem_bytes(N);
     int per_sm = 0;
     MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -548,7 +542,18 @@ void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out)
     MCQ_CUDA(cudaGetLastError());
 }
 
-// A bounded device wait that gave up leaves MCQ_ERR_TIMEOUT in the workspace's error word.
+// A bounded device wait that gave up leaves MCQ_ERR_TIMEOUT in the workspace's error word.  The
+// word is cleared only when it is armed afresh after a check, so a failure of an asynchronous pass
+// stays there until the next synchronous call on the workspace reads it.
+int* arm_err_word(Workspace& ws) {
+    int* err = (int*)ws.err.ensure(sizeof(int));
+    if (!ws.err_armed) {
+        MCQ_CUDA(cudaMemsetAsync(err, 0, sizeof(int), ws.stream));
+        ws.err_armed = true;
+    }
+    return err;
+}
+
 void check_err_word(Workspace& ws) {
     if (!ws.err_armed) return;
     int h = 0;

@@ -159,6 +159,9 @@ std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
 // After a synchronisation of ws.stream: raises MCQ_ERR_TIMEOUT if a bounded device-side wait of
 // the workspace's last tensor-core or assisted pass gave up.
 void check_err_word(Workspace& ws);
+// The workspace's error word for a pass with bounded device waits (cleared unless it still holds
+// an unread status of an earlier asynchronous pass).
+int* arm_err_word(Workspace& ws);
 // Occupancy / shared-memory set-up of a kernel for a dynamic shared-memory size (cached).
 KernelInfo& kernel_info(const void* fn, size_t smem);
 // Pathwise adjoint Greeks over R scrambled replicas (k_adjoint.cu).

@@ -293,7 +293,10 @@ int mcq_qmc_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, int noise
                  mcq_handle bb, mcq_handle pca, uint32_t salt_base, int R, uint32_t offset,
                  int64_t n_points, int flags, double* sums_host);
 /* Same pass with device-resident output (sums_device: R*2 doubles) on `stream`;
-   asynchronous.  Used to time the kernel with inputs and outputs resident in HBM. */
+   asynchronous.  Used to time the kernel with inputs and outputs resident in HBM.  A bounded
+   device-side wait that gives up in such a pass (MCQ_ERR_TIMEOUT) is reported by the next
+   synchronous call on the engine's default workspace (mcq_qmc_pass, mcq_level_pass, mcq_run_qmc,
+   mcq_run_mc). */
 int mcq_qmc_pass_device(const mcq_model* m, const mcq_payoff* p, int n_steps, int noise_mode,
                         mcq_handle bb, mcq_handle pca, uint32_t salt_base, int R,
                         uint32_t offset, int64_t n_points, int flags, double* sums_device,
