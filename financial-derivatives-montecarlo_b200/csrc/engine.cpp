@@ -501,7 +501,9 @@ void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out)
     const uint64_t G = ((a.offset + a.n_points - 1) >> 5) - g0 + 1;
     const uint64_t gpt = (uint64_t)pca_tile_paths() / 32;   // 32-point groups per tile
     const uint64_t tiles = (G + gpt - 1) / gpt;
-    const uint64_t target = 148ULL * 4;
+    // about 32 items per CTA (one CTA per SM): with four, the CTA that drew a fifth item set the
+    // kernel's length (a fifth of the pass idle at the tail)
+    const uint64_t target = 148ULL * 32;
     uint64_t tpi = (tiles * (uint64_t)a.R + target - 1) / target;
     if (tpi < 1) tpi = 1;
     const uint64_t ipr = (tiles + tpi - 1) / tpi;
