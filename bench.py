@@ -88,15 +88,23 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
-        if not self.rows:
+    def wait_rows(self, n, timeout):
+        """Wait (at most `timeout` s) until at least n samples have arrived; nvidia-smi takes a
+        while to start, longer than a short timed region."""
+        t0 = time.time()
+        while self.proc and len(self.rows) < n and time.time() - t0 < timeout:
+            time.sleep(0.01)
+
+    def summary(self, first=0):
+        rows = self.rows[first:]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
-        mx = max((float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()), default=None)
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max((float(r[2]) for r in rows if r[2].replace(".", "").isdigit()), default=None)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(self.rows)}
+                "samples": len(rows)}
 
 
 def measured_peaks():
@@ -338,21 +346,28 @@ def main():
     def one_pass():
         eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, salt_base=salt, R=REPS, offset=0, n_points=N)
 
+    # the clock sampler starts before the warm-up (nvidia-smi needs a moment to start) and its
+    # summary keeps the samples from the start of the timed region on
+    clk = ClockSampler(local_rank).__enter__()
     for _ in range(args.warmup):
         flush.zero_()
         one_pass()
     torch.cuda.synchronize()
+    clk.wait_rows(1, 10.0)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(local_rank) as clk:
-        for i in range(args.steps):
-            flush.zero_()
-            evs[i][0].record(stream)
-            one_pass()
-            evs[i][1].record(stream)
-        torch.cuda.synchronize()
+    clk_first = len(clk.rows)
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        one_pass()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    clk.wait_rows(clk_first + 1, 2.0)   # at least the sample that closes the timed region
+    clocks = clk.summary(clk_first)
+    clk.__exit__(None, None, None)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -422,7 +437,6 @@ def main():
         return
 
     peaks = measured_peaks()
-    clocks = clk.summary()
     sm_count = torch.cuda.get_device_properties(local_rank).multi_processor_count
     mhz = clocks["sm_mhz"] or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or 1965.0
     peak_fp32 = sm_count * 128 * 2 * mhz * 1e6 / 1e12

@@ -142,8 +142,8 @@ struct PassArgs {
 // B200 at four CTAs per SM: a warp's last item then costs at most an eighth of the pass (with
 // three per warp the small first passes of the adaptive drivers lost up to a quarter).
 inline constexpr long long kTargetItems = 148LL * 32 * 8;
-// the adjoint's split (two CTAs per SM, checkpoint state per warp)
-inline constexpr long long kTargetItemsAdjoint = 148LL * 16 * 3;
+// the adjoint's split: about eight items per resident warp (two CTAs of eight warps per SM)
+inline constexpr long long kTargetItemsAdjoint = 148LL * 16 * 8;
 
 int noise_dim(const mcq_model& m);
 // KParams for a pass (make_params); basket / local-vol arrays are uploaded into ws.aux.
