@@ -40,7 +40,7 @@ constexpr int kBookMaxR = 32;
 constexpr int kBookClasses = 4;            // basket width 1-4, 5-8, 9-12, 13-16
 constexpr int kChunkNormals = 8192;        // normals per lane a chunk aims at
 constexpr int kMinChunksPerRep = 64;
-constexpr int kMaxChunksPerRep = 256;
+constexpr int kMaxChunksPerRep = 1024;
 
 // hdr (int32): [0] n_specs, [1] n_chunks, [2 + c] first chunk of class c, [6] = n_chunks,
 // [7 + c] first slice of class c, [11] = n_specs, [12 + c] work-queue counter of class c.
