@@ -266,7 +266,7 @@ __device__ __forceinline__ void heston_adj_step(const KParams& p, float& S, floa
     const float sq = sqrtf(fmaxf(V, 0.f));
     S = fmaf(S, fmaf(sq, dw1, muh), S);
     V = fmaf(p.xi * sq, dw2, fmaf(p.em_f, V - p.theta, p.theta));
-    if (p.mil != 0.f) V = fmaf(p.mil, dw2 * dw2, V - p.mil_hf);
+    V = fmaf(p.mil, dw2 * dw2, V - p.mil_hf);   // Milstein term; without the flag mil = mil_hf = 0
 }
 
 template <int PAY>

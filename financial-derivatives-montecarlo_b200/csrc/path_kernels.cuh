@@ -269,6 +269,13 @@ struct Leg {
         else if constexpr (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) r0 = fminf(r0, S);
         else if constexpr (PAY == PAY_UPOUT) r0 = fmaxf(r0, S);
     }
+    // update() when `on`, as selects rather than a branch per step (the same values)
+    __device__ __forceinline__ void update_if(bool on) {
+        if constexpr (PAY == PAY_ASIAN) tp += on ? S : 0.f;
+        else if constexpr (PAY == PAY_GEOM) { if (on) tp += logf(S); }
+        else if constexpr (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) r0 = on ? fminf(r0, S) : r0;
+        else if constexpr (PAY == PAY_UPOUT) r0 = on ? fmaxf(r0, S) : r0;
+    }
     template <bool RUN>
     __device__ __forceinline__ void step(const KParams& p, float dw1, float dw2, float t,
                                          float muh, float em, float milh) {
@@ -284,7 +291,9 @@ struct Leg {
             const float sq = sqrtf(fmaxf(V, 0.f));
             S = fmaf(S, fmaf(sq, dw1, muh), S);
             V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
-            if (p.mil != 0.f) V = fmaf(p.mil, dw2 * dw2, V - milh);   // Milstein: xi^2/4 (dW^2 - h)
+            // Milstein: xi^2/4 (dW^2 - h); without the flag mil = milh = 0 and this leaves V as it
+            // is, so it runs unconditionally (no branch per step)
+            V = fmaf(p.mil, dw2 * dw2, V - milh);
         }
         if constexpr (RUN && path_dep<PAY>()) update();
     }
@@ -326,16 +335,24 @@ struct PathC {
     }
     __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
         const float t = (float)k * p.h;
-        if (run_upd) f.template step<true>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
-        else f.template step<false>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
+        if constexpr (HES && COUPLED) {   // run_upd is a runtime flag only here
+            f.template step<false>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
+            if constexpr (path_dep<PAY>()) f.update_if(run_upd);
+        } else {
+            f.template step<true>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
+        }
         k++;
         if constexpr (COUPLED) {
             a1 += dw1;
             if constexpr (HES) a2 += dw2;
             if (++m == p.M) {
                 const float tc = (float)ck * p.hc;
-                if (run_upd) c.template step<true>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
-                else c.template step<false>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
+                if constexpr (HES) {
+                    c.template step<false>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
+                    if constexpr (path_dep<PAY>()) c.update_if(run_upd);
+                } else {
+                    c.template step<true>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
+                }
                 a1 = a2 = 0.f; m = 0; ck++;
             }
         }
