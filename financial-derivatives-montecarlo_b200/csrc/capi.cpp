@@ -402,6 +402,10 @@ int mcq_qmc_pass_device(const mcq_model* m, const mcq_payoff* p, int n_steps, in
         ws.stream = user;
         try { pass_async(ws, a, sums_device); } catch (...) { ws.stream = own; throw; }
         ws.stream = own;
+        // the workspace's scratch and status word were used on the caller's stream: later work
+        // on the workspace (the next pass, the status read of the next synchronous call) waits
+        // for this pass
+        join_caller_stream(ws, user);
     } else {
         pass_async(ws, a, sums_device);
     }

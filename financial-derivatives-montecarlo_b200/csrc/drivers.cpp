@@ -77,6 +77,7 @@ void run_mc(const mcq_model& m, const mcq_payoff& p, double eps, int n_steps,
     out.path_steps = ps;
     out.levels = 1;
     out.launches = engine().launches - l0;
+    out.converged = 1;
 }
 
 void run_mc_fixed(const mcq_model& m, const mcq_payoff& p, int n_steps, long long n_paths,
@@ -164,6 +165,7 @@ void run_qmc(const mcq_model& m, const mcq_payoff& p, double eps, int n_steps,
     out.path_steps = ps;
     out.levels = 1;
     out.launches = engine().launches - l0;
+    out.converged = (vom < eps * eps / 2.0) ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ MLMC
@@ -277,6 +279,7 @@ void run_mlmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_mlm
     out.path_steps = ps;
     out.levels = L + 1;
     out.launches = engine().launches - l0c;
+    out.converged = converged ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ MLQMC
@@ -419,6 +422,7 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
     out.path_steps = ps;
     out.levels = L + 1;
     out.launches = engine().launches - l0c;
+    out.converged = converged ? 1 : 0;
 }
 
 // ------------------------------------------------------------------ control variates
@@ -477,6 +481,7 @@ void run_mc_cv(const mcq_model& main_m, const mcq_payoff& main_p, double E_ctrl,
     out.path_steps = (double)(cfg.pilot_n + N) * n_steps;
     out.levels = 1;
     out.launches = engine().launches - l0c;
+    out.converged = 1;
 }
 
 // run_qmc_cv_cuda (methods_cuda.cu:2165-2278)
@@ -537,6 +542,7 @@ void run_qmc_cv(const mcq_model& main_m, const mcq_payoff& main_p, double E_ctrl
     out.path_steps = ps;
     out.levels = 1;
     out.launches = engine().launches - l0c;
+    out.converged = 1;
 }
 
 // ------------------------------------------------------------------ importance sampling
@@ -573,6 +579,7 @@ void run_is(const mcq_model& gbm, const mcq_payoff& eur, double z_star, double e
     out.path_steps = (double)(cfg.pilot_n + N) * n_steps;
     out.levels = 1;
     out.launches = engine().launches - l0c;
+    out.converged = 1;
 }
 
 }  // namespace mcq

@@ -59,7 +59,14 @@ void Workspace::ensure_stream() {
     if (!stream) MCQ_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 }
 Workspace::~Workspace() {
+    if (joined) cudaEventDestroy(joined);
     if (stream) cudaStreamDestroy(stream);
+}
+
+void join_caller_stream(Workspace& ws, cudaStream_t caller) {
+    if (!ws.joined) MCQ_CUDA(cudaEventCreateWithFlags(&ws.joined, cudaEventDisableTiming));
+    MCQ_CUDA(cudaEventRecord(ws.joined, caller));
+    MCQ_CUDA(cudaStreamWaitEvent(ws.stream, ws.joined, 0));
 }
 
 // ------------------------------------------------------------------ engine
@@ -558,10 +565,13 @@ int* arm_err_word(Workspace& ws) {
 
 void check_err_word(Workspace& ws) {
     if (!ws.err_armed) return;
-    int h = 0;
-    MCQ_CUDA(cudaMemcpy(&h, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    // read on the workspace stream, which a pass on a caller's stream has been joined into
+    // (join_caller_stream), so the word is read after every pass that may have set it
+    int* h = (int*)ws.haux.ensure(sizeof(int));
+    MCQ_CUDA(cudaMemcpyAsync(h, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, ws.stream));
+    MCQ_CUDA(cudaStreamSynchronize(ws.stream));
     ws.err_armed = false;
-    MCQ_REQUIRE(h == 0, MCQ_ERR_TIMEOUT, "a bounded device-side wait timed out (status " + std::to_string(h) + ")");
+    MCQ_REQUIRE(*h == 0, MCQ_ERR_TIMEOUT, "a bounded device-side wait timed out (status " + std::to_string(*h) + ")");
 }
 
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a) {

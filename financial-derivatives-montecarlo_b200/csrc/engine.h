@@ -49,9 +49,13 @@ struct PinnedBuf {
 };
 
 // Scratch owned by one stream: item partials, per-replica sums, scrambled direction words,
-// small parameter uploads.  Launches on one workspace are ordered by its stream.
+// small parameter uploads.  Launches on one workspace are ordered by its stream; a pass run on a
+// caller's stream is joined back into it (`joined`, recorded on the caller's stream and waited
+// on by the workspace stream), so later work on the workspace, and the read of its status word,
+// comes after that pass.
 struct Workspace {
     cudaStream_t stream = nullptr;
+    cudaEvent_t joined = nullptr;
     DevBuf partials, sums, dirs, aux, dump, err;
     bool err_armed = false;   // err holds a fresh status from the last tensor-core pass
     PinnedBuf hsums, haux;
@@ -159,6 +163,8 @@ std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
 // After a synchronisation of ws.stream: raises MCQ_ERR_TIMEOUT if a bounded device-side wait of
 // the workspace's last tensor-core or assisted pass gave up.
 void check_err_word(Workspace& ws);
+// Orders the workspace stream after everything issued so far on `caller`.
+void join_caller_stream(Workspace& ws, cudaStream_t caller);
 // The workspace's error word for a pass with bounded device waits (cleared unless it still holds
 // an unread status of an earlier asynchronous pass).
 int* arm_err_word(Workspace& ws);

@@ -264,9 +264,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
 __device__ __forceinline__ void heston_adj_step(const KParams& p, float& S, float& V, float dw1, float dw2,
                                                 float muh) {
     const float sq = sqrtf(fmaxf(V, 0.f));
-    S = fmaf(S, fmaf(sq, dw1, muh), S);
+    S = fmaf(sq * S, dw1, fmaf(muh, S, S));   // the pricing pass's operations (Leg::step)
     V = fmaf(p.xi * sq, dw2, fmaf(p.em_f, V - p.theta, p.theta));
-    V = fmaf(p.mil, dw2 * dw2, V - p.mil_hf);   // Milstein term; without the flag mil = mil_hf = 0
+    // Milstein term only with the flag (mil != 0): fmaf(0, dW^2, V) would turn an infinite
+    // normal (reference-compat u = 1 point) into NaN
+    V = (p.mil != 0.f) ? fmaf(p.mil, dw2 * dw2, V - p.mil_hf) : V;
 }
 
 template <int PAY>

@@ -19,10 +19,17 @@
 // Two calls whose work overlaps on the GPU (for example on two streams at once) race on the
 // array and produce wrong sums; issue them on one stream or synchronise in between.
 //
-// Set-up: the first call on each device (with that device current) resolves the array's
-// device address with cudaGetSymbolAddress and copies the JoeKuo direction table for the first
-// kMaxDims dimensions into it (a synchronous cudaMemcpy).  That first call should therefore
+// Set-up: every call resolves the array's device address with cudaGetSymbolAddress for the
+// current device (a host-side lookup, no allocation).  The first call on each device, and the
+// first call in a new context of that device (after a cudaDeviceReset the library's module and
+// this array are loaded afresh, empty), copies the JoeKuo direction table for the first kMaxDims
+// dimensions into the array with a synchronous cudaMemcpy.  That first call should therefore
 // come before any stream capture.
+//
+// Work split and kernels: those of mcq_qmc_pass_device for the same request (the plain raw
+// pass, or the packed pass with its whole-tile items for paths of at most 16 normals), so both
+// entry points give the same sums bit for bit.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <curand.h>
 
@@ -54,21 +61,48 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-unsigned char* g_scratch[kMaxDevices] = {};   // device address of g_noalloc_scratch per device
+unsigned char* g_scratch[kMaxDevices] = {};      // device address the table was loaded at
+unsigned long long g_ctx_id[kMaxDevices] = {};   // context it was loaded in (driver context id)
 int g_sm_count[kMaxDevices] = {};
 
-// Once per device, with that device current: resolve the array's device address (the host-side
-// name g_noalloc_scratch is only a stand-in and must never be passed to a kernel) and load the
-// direction table.
+// The driver's id of the current context (unique for the life of the process: a context
+// created after a cudaDeviceReset has a new id), through the runtime's driver entry points.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        MCQ_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q));
+        MCQ_REQUIRE(f && q == cudaDriverEntryPointSuccess, MCQ_ERR_CUDA, "cuCtxGetCurrent not available");
+        get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        MCQ_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q));
+        MCQ_REQUIRE(f && q == cudaDriverEntryPointSuccess, MCQ_ERR_CUDA, "cuCtxGetId not available");
+        get_id = reinterpret_cast<GetId>(f);
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    MCQ_REQUIRE(get_current(&c) == CUDA_SUCCESS && c != nullptr, MCQ_ERR_CUDA, "no current CUDA context");
+    MCQ_REQUIRE(get_id(c, &id) == CUDA_SUCCESS, MCQ_ERR_CUDA, "cuCtxGetId failed");
+    return id;
+}
+
+// Every call, with the device current: resolve the array's device address (the host-side name
+// g_noalloc_scratch is only a stand-in and must never be passed to a kernel), and load the
+// direction table when this device's array has not been loaded in this context at this address.
 unsigned char* scratch_for_current_device(int* sm_count) {
     int dev = -1;
     MCQ_CUDA(cudaGetDevice(&dev));
     MCQ_REQUIRE(dev >= 0 && dev < kMaxDevices, MCQ_ERR_RANGE, "device index beyond the set-up table");
+    void* ptr = nullptr;
+    MCQ_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    MCQ_REQUIRE(ptr != nullptr, MCQ_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch[dev]) {
-        void* ptr = nullptr;
-        MCQ_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-        MCQ_REQUIRE(ptr != nullptr, MCQ_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+    if (g_scratch[dev] != ptr || g_ctx_id[dev] != ctx) {
         curandDirectionVectors32_t* hv = nullptr;
         MCQ_REQUIRE(curandGetDirectionVectors32(&hv, CURAND_DIRECTION_VECTORS_32_JOEKUO6) ==
                         CURAND_STATUS_SUCCESS,
@@ -78,6 +112,7 @@ unsigned char* scratch_for_current_device(int* sm_count) {
         MCQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         g_sm_count[dev] = sms;
         g_scratch[dev] = static_cast<unsigned char*>(ptr);
+        g_ctx_id[dev] = ctx;
     }
     *sm_count = g_sm_count[dev];
     return g_scratch[dev];
@@ -108,18 +143,27 @@ static void qmc_pass_noalloc(const mcq_model* m, const mcq_payoff* p, int n_step
     KParams k;
     fill_params(unused, a, k);
 
+    // the kernel and work split of mcq_qmc_pass_device for this request (engine.cpp pass_async):
+    // paths of at most 16 normals take the packed pass, whose items are whole tiles of 32 / D
+    // groups; the plain pass otherwise (the assisted form it may choose for few long paths gives
+    // the plain pass's bits)
+    const void* fn = (D <= 16) ? lookup_sobol_packed(k.model, p->kind, false) : nullptr;
+    const bool packed = fn != nullptr;
+    if (!fn) fn = lookup_pass(GEN_SOBOL, NOISE_RAW, EST_PLAIN, k.model, p->kind, 0);
+    MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no fused kernel for this model / payoff");
     const uint64_t g0 = a.offset >> 5;
     const uint64_t G = ((a.offset + a.n_points - 1) >> 5) - g0 + 1;
     uint64_t gpi = (G * (uint64_t)R + kTargetItems - 1) / kTargetItems;
     if (gpi < 1) gpi = 1;
+    if (packed) {
+        const uint64_t Q = (uint64_t)(32 / D);
+        gpi = (gpi + Q - 1) / Q * Q;
+    }
     const uint64_t ipr = (G + gpi - 1) / gpi;
     MCQ_REQUIRE(ipr * (uint64_t)R <= (uint64_t)kMaxItems, MCQ_ERR_RANGE,
                 "work split needs more than " + std::to_string(kMaxItems) + " items");
     k.R = R; k.gpi = (int)gpi; k.items_per_rep = (int)ipr; k.n_items = (int)(ipr * R);
     k.offset = a.offset; k.n_points = a.n_points; k.g0 = g0; k.G = G;
-
-    const void* fn = lookup_pass(GEN_SOBOL, NOISE_RAW, EST_PLAIN, k.model, p->kind, 0);
-    MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no fused kernel for this model / payoff");
 
     int sms = 0;
     unsigned char* base = scratch_for_current_device(&sms);

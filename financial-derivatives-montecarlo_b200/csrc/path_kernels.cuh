@@ -288,12 +288,17 @@ struct Leg {
             const float sl = lv_sigma(p, S, t);
             S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_HESTON) {
+            // S + mu h S + (sqrt(V+) S) dW1 with the reference's product sqrt(V+) S (:280): a path
+            // that went infinite (reference-compat u = 1 point) and whose variance truncates to 0
+            // then becomes NaN (0 * inf) as the reference's does, not +inf
             const float sq = sqrtf(fmaxf(V, 0.f));
-            S = fmaf(S, fmaf(sq, dw1, muh), S);
+            S = fmaf(sq * S, dw1, fmaf(muh, S, S));
             V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
-            // Milstein: xi^2/4 (dW^2 - h); without the flag mil = milh = 0 and this leaves V as it
-            // is, so it runs unconditionally (no branch per step)
-            V = fmaf(p.mil, dw2 * dw2, V - milh);
+            // Milstein: xi^2/4 (dW^2 - h), selected by the parameter block (a uniform predicate,
+            // no branch per step).  Without the flag V is kept as it is: an unconditional
+            // fmaf(0, dW^2, V) would turn the +inf normal of the reference-compat u = 1 point
+            // into NaN, where the reference's Euler step keeps V = +inf.
+            V = (p.mil != 0.f) ? fmaf(p.mil, dw2 * dw2, V - milh) : V;
         }
         if constexpr (RUN && path_dep<PAY>()) update();
     }

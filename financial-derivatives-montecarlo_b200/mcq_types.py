@@ -55,7 +55,7 @@ class MLMCCfg(C.Structure):
 class Result(C.Structure):
     _fields_ = [("price", C.c_double), ("std_error", C.c_double), ("n_samples", C.c_int64),
                 ("time_s", C.c_double), ("path_steps", C.c_double), ("levels", C.c_int32),
-                ("launches", C.c_int32)]
+                ("launches", C.c_int32), ("converged", C.c_int32), ("reserved", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -139,6 +139,11 @@ typedef struct mcq_result {
     double  path_steps;           /* total simulated path-steps (fine + coarse for MLMC) */
     int32_t levels;               /* MLMC/MLQMC: L + 1 */
     int32_t launches;             /* engine kernel launches issued */
+    int32_t converged;            /* 1: the driver's stopping test passed (MLMC/MLQMC: the bias
+                                     test before the iteration cap, :1473 / :1999; QMC: var of
+                                     the replica means < eps^2/2 before the doubling cap); MC, CV
+                                     and IS size N from the pilot and always report 1 */
+    int32_t reserved;
 } mcq_result;
 
 /* CVPilot (methods_cuda.cuh:94). */
@@ -320,10 +325,12 @@ int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, i
  * device.  Its scratch is one fixed __device__ array inside the library (about 2.7 MiB, held on
  * every GPU that loads the library until exit); sums_device ([R][2] doubles) is the caller's.
  * Limits: GBM, Heston or parametric Dupire, raw ordering, n_steps x factors <= 512, R <= 32;
- * larger requests fail with MCQ_ERR_RANGE.  The first call on a device sets the array up
- * (resolves its address, loads the direction table with a synchronous copy) and should come
- * before any stream capture.  All calls share the array: calls that overlap on the GPU race,
- * so keep them on one stream.  Asynchronous on `stream` (NULL: the legacy default stream). */
+ * larger requests fail with MCQ_ERR_RANGE.  Same kernel and work split as mcq_qmc_pass_device,
+ * hence the same sums bit for bit.  The first call on a device (and the first in a new context of
+ * it, e.g. after cudaDeviceReset) loads the direction table into the array with a synchronous
+ * copy and should come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so keep them on one stream.  Asynchronous on `stream` (NULL: the
+ * legacy default stream). */
 int mcq_qmc_pass_noalloc(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t salt_base,
                          int R, uint32_t offset, int64_t n_points, int flags, double* sums_device,
                          void* stream);

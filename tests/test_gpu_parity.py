@@ -210,3 +210,49 @@ def test_heston_milstein_flag(gpu, orc, pay):
     for r in range(R):
         for k in (0, 2):
             assert abs(gl[r, k] / N - ol[r, k] / N) < tol(pay, N, ol[r, k] / N) * 2, (r, k, gl[r], ol[r])
+
+
+
+def _top_points(orc, salt, dims, n=1 << 22):
+    """First point index per dimension whose scrambled word is >= 0xFFFFFF80 (u rounds to 1)."""
+    out = {}
+    for dim in dims:
+        hit = np.nonzero(orc.sobol_hh_u32(salt, dim, 1, 0, n)[0] >= 0xFFFFFF80)[0]
+        if len(hit):
+            out[dim] = int(hit[0])
+    return out
+
+
+@pytest.mark.parametrize("parity", [0, 1])
+@pytest.mark.parametrize("pay", ["eur", "lookback"])
+def test_heston_compat_u_inf_matches_reference(gpu, orc, parity, pay):
+    """Under MCQ_FLAG_COMPAT_U_INF a scrambled word >= 0xFFFFFF80 gives u = 1 and an infinite
+    normal (methods_cuda.cu:823).  In the reference's Heston step (:276-284) that normal makes
+    S or V infinite, a truncated variance then gives 0 * inf = NaN in S, and fmaxf drops the NaN
+    in the payoff.  The engine must take the same path to the same sums (oracle = the reference's
+    formulas in FP64), for a hit on the first (z1, even dimension) and the second (z2, odd
+    dimension) normal of a step, single level and coupled; in particular the Milstein term must
+    not turn an infinite variance into NaN when it is off.  The default mode stays finite."""
+    m, p = make_model(gpu, "heston"), make_payoff(gpu, pay)
+    hits = _top_points(orc, 42, [d for d in range(64) if d % 2 == parity])
+    assert hits
+    dim, x = min(hits.items(), key=lambda kv: kv[0])
+    off, N, C = (x // 32) * 32, 32, gpu.FLAG_COMPAT_U_INF
+
+    def same(a, b):
+        fa, fb = np.isfinite(a), np.isfinite(b)
+        if fa != fb:
+            return False
+        return (not fa) or abs(a / N - b / N) < tol(pay, N, b / N)
+
+    g = gpu.qmc_pass(m, p, 32, salt_base=42, R=1, offset=off, n_points=N, flags=C)
+    o = orc.qmc_sums(m, p, 32, None, salt_base=42, R=1, offset=off, N=N, flags=C)
+    o0 = orc.qmc_sums(m, p, 32, None, salt_base=42, R=1, offset=off, N=N)
+    if pay == "lookback":
+        assert np.isnan(o[0, 0])                  # the NaN path reaches the lookback payoff
+    assert same(g[0, 0], o[0, 0]), (dim, g, o)
+    gl = gpu.level_pass(m, p, 32, 4, use_sobol=True, salt_base=42, R=1, offset=off, n_points=N, flags=C)
+    ol = orc.level_sums(m, p, 32, 4, None, use_sobol=True, salt_base=42, R=1, offset=off, N=N, flags=C)
+    assert same(gl[0, 2], ol[0, 2]) and same(gl[0, 0], ol[0, 0]), (dim, gl, ol)
+    g0 = gpu.qmc_pass(m, p, 32, salt_base=42, R=1, offset=off, n_points=N)
+    assert np.isfinite(g0[0, 0]) and abs(g0[0, 0] / N - o0[0, 0] / N) < tol(pay, N, o0[0, 0] / N)

@@ -64,3 +64,30 @@ def test_noalloc_heston_and_limits(eng):
     with pytest.raises(eng.MCQError) as e:
         eng.qmc_pass_noalloc(eng.gbm(), p, 64, out.data_ptr(), 0, R=33, n_points=64)
     assert e.value.code == 4
+
+
+@pytest.mark.parametrize("model,pay,n_steps", [
+    ("dupire", "eur", 64),      # parametric Dupire, plain pass
+    ("dupire", "asian", 300),   # long paths: the allocating entry point may take its assisted form
+    ("gbm", "asian", 8),        # 8 normals a path: the packed pass with whole-tile work items
+    ("heston", "eur", 4),       # 2 factors x 4 steps = 8 normals: packed as well
+    ("gbm", "eur", 16),         # the packed limit
+])
+def test_noalloc_models_and_short_paths(eng, model, pay, n_steps):
+    """Parametric Dupire and paths of at most 16 normals (where the allocating pass switches to
+    its packed kernel) give the allocating entry point's sums bit for bit, twice in a row."""
+    import torch
+    m = {"gbm": lambda: eng.gbm(100.0, 0.03, 0.25, 1.0),
+         "dupire": lambda: eng.dupire(100.0, 0.05, 0.2, 0.5, 0.7, 1.0),
+         "heston": lambda: eng.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)}[model]()
+    p = eng.european(100.0, 0.05, 1.0) if pay == "eur" else eng.asian(100.0)
+    R = 4
+    out = torch.zeros(2 * R, dtype=torch.float64, device="cuda")
+    ref = torch.zeros(2 * R, dtype=torch.float64, device="cuda")
+    for salt, off, n in ((11, 0, 40000), (12, 777, 5000)):
+        eng.qmc_pass_noalloc(m, p, n_steps, out.data_ptr(), 0, salt_base=salt, R=R, offset=off, n_points=n)
+        eng.qmc_pass_device(m, p, n_steps, ref.data_ptr(), 0, salt_base=salt, R=R, offset=off, n_points=n)
+        torch.cuda.synchronize()
+        a, b = out.cpu().numpy(), ref.cpu().numpy()
+        assert np.array_equal(a, b), (model, n_steps, salt, a, b)
+        assert np.all(np.isfinite(a)) and np.all(a[0::2] > 0)
