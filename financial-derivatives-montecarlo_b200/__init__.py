@@ -26,7 +26,7 @@ EXPORTS = [
     "mcq_bb_create", "mcq_pca_create", "mcq_pca_create_from", "mcq_handle_free", "mcq_handle_info",
     "mcq_run_mc", "mcq_run_mc_fixed", "mcq_run_qmc", "mcq_run_mlmc", "mcq_run_mlqmc", "mcq_cv_pilot",
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
-    "mcq_mc_pass", "mcq_level_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
+    "mcq_mc_pass", "mcq_level_pass", "mcq_is_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
     "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_debug_wait_timeout", "mcq_qmc_pass_noalloc",
     "mcq_adjoint",
     "mcq_book_price", "mcq_book_level_sums", "mcq_book_create", "mcq_book_submit", "mcq_book_size",
@@ -345,6 +345,17 @@ def level_pass(m, p, n_fine, M, noise=RAW, bb=None, pca=None, use_sobol=True, se
                                 _h(pca), C.c_int(int(use_sobol)), C.c_uint32(seed), C.c_uint32(salt_base),
                                 C.c_int(R), C.c_uint32(offset), C.c_int64(n_points), C.c_int(flags),
                                 out.ctypes.data_as(_P(C.c_double))))
+    return out
+
+
+def is_pass(m, p, n_steps, z_star_step, use_sobol=True, seed=42, salt_base=42, R=1, offset=0, n_points=1024,
+            flags=0):
+    """Importance-sampling pass (kernel_is_gbm): [R][2] {sum Y, sum Y^2}; z_star_step per step."""
+    out = np.zeros((R, 2), np.float64)
+    _check(lib().mcq_is_pass(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_double(z_star_step),
+                             C.c_int(int(use_sobol)), C.c_uint32(seed), C.c_uint32(salt_base), C.c_int(R),
+                             C.c_uint32(offset), C.c_int64(n_points), C.c_int(flags),
+                             out.ctypes.data_as(_P(C.c_double))))
     return out
 
 

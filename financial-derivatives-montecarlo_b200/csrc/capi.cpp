@@ -449,6 +449,26 @@ int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, i
     API_END
 }
 
+int mcq_is_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star_step, int use_sobol,
+                uint32_t seed, uint32_t salt_base, int R, uint32_t offset, int64_t n_points, int flags,
+                double* sums_host) {
+    API_BEGIN
+    NEED(m); NEED(p); NEED(sums_host);
+    MCQ_REQUIRE(m->kind == MCQ_MODEL_GBM && p->kind == MCQ_PAYOFF_EUROPEAN, MCQ_ERR_UNSUPPORTED,
+                "IS pass: GBM with a European call only (kernel_is_gbm)");
+    MCQ_REQUIRE(R >= 1 && n_points >= 0 && n_steps >= 1, MCQ_ERR_INVALID, "bad IS pass sizes");
+    PassArgs a;
+    a.m = m; a.p = p; a.n_steps = n_steps; a.est = EST_IS;
+    a.gen = use_sobol ? GEN_SOBOL : GEN_PHILOX;
+    a.seed = seed; a.salt0 = salt_base; a.stream0 = salt_base; a.R = R;
+    a.offset = offset; a.n_points = (uint64_t)n_points; a.flags = flags;
+    a.z_star = (float)z_star_step;
+    ensure_ready();
+    auto s = pass_sync(engine().ws(0), a);
+    std::memcpy(sums_host, s.data(), sizeof(double) * 2 * R);
+    API_END
+}
+
 int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_handle bb,
                         int use_sobol, uint32_t seed, uint32_t salt_base, int R, uint32_t offset,
                         int64_t n_points, int flags, float* out_host) {

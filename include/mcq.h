@@ -318,6 +318,15 @@ int mcq_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, i
                    uint32_t salt_base, int R, uint32_t offset, int64_t n_points, int flags,
                    double* sums_host);
 
+/* Importance-sampling pass (kernel_is_gbm, methods_cuda.cu:685-707): GBM European paths under
+   the drift shift z_star_step per step (run_is_cuda passes z_star / sqrt(n_steps), :2297),
+   payoff times the likelihood ratio; sums_host[R][2] = {sum Y, sum Y^2}.  use_sobol=1:
+   scrambled Sobol with salts salt_base + r from point `offset`; 0: Philox key `seed`, stream
+   salt_base + r.  The unit behind mcq_run_is (which uses Philox). */
+int mcq_is_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star_step, int use_sobol,
+                uint32_t seed, uint32_t salt_base, int R, uint32_t offset, int64_t n_points, int flags,
+                double* sums_host);
+
 /* One RQMC pass (as mcq_qmc_pass_device) that allocates no device memory.  No counterpart in
  * the reference.  For callers that may not call cudaMalloc: code living in a process whose GPU
  * memory belongs to another allocator (a framework's caching allocator, a plugin host with a

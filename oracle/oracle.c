@@ -856,6 +856,78 @@ int orc_mc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t s
     return 0;
 }
 
+/* kernel_is_gbm (methods_cuda.cu:685-707) in FP64: one GBM European path under the drift-shifted
+ * measure Z' = Z + z*, with the likelihood ratio exp(-z* sum Z - n z*^2 / 2); z_star is the
+ * per-step shift the kernel reads (run_is_cuda passes z_star / sqrt(n_steps), :2297). */
+double orc_is_payoff(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star, const double* z) {
+    double h = m->T / n_steps, sh = sqrt(h), S = m->S0, zs = 0.0;
+    for (int k = 0; k < n_steps; k++) {
+        zs += z[k];
+        double dw = (z[k] + z_star) * sh;
+        S = S + m->mu * S * h + m->sigma * S * dw;
+    }
+    double lr = exp(-z_star * zs - 0.5 * z_star * z_star * n_steps);
+    return fmax(S - p->K, 0.0) * pay_discount(p) * lr;
+}
+
+/* IS sums {sum Y, sum Y^2} per replica: scrambled Sobol (salts salt_base + r, points offset ..
+ * offset + N - 1) or Philox (key seed, stream salt_base + r, paths offset ..). */
+int orc_is_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star, int use_sobol,
+                uint32_t seed, uint32_t salt_base, int R, uint32_t offset, int64_t N, int flags,
+                int n_threads, double* sums) {
+    int D = n_steps;
+    if (use_sobol && D > 20000) return -1;
+    if (use_sobol && (uint64_t)offset + (uint64_t)N > 0x100000000ull) return -2;
+    int nch = (N < ORC_CHUNKS) ? (int)(N > 0 ? N : 1) : ORC_CHUNKS;
+    double* part = (double*)calloc((size_t)R * nch * 2, sizeof(double));
+    uint32_t* Lv = NULL;
+    if (use_sobol) {
+        Lv = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)R * D * 33);
+        for (int r = 0; r < R; r++)
+            for (int dd = 0; dd < D; dd++) {
+                uint32_t* w = Lv + ((size_t)r * D + dd) * 33;
+                prescramble(salt_base + (uint32_t)r, dd, w, w + 32);
+            }
+    }
+    int nt = n_threads > 0 ? n_threads : orc_max_threads();
+    (void)nt;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int64_t task = 0; task < (int64_t)R * nch; task++) {
+        int r = (int)(task / nch), c = (int)(task % nch);
+        int64_t b = N * c / nch, e = N * (c + 1) / nch;
+        if (b >= e) continue;
+        uint32_t* x = (uint32_t*)malloc(sizeof(uint32_t) * D);
+        double* z = (double*)malloc(sizeof(double) * (D + 4));
+        const uint32_t* L = use_sobol ? Lv + (size_t)r * D * 33 : NULL;
+        if (use_sobol)
+            for (int dd = 0; dd < D; dd++) x[dd] = scr_direct(L + dd * 33, L[dd * 33 + 32], offset + (uint32_t)b);
+        double s1 = 0, s2 = 0;
+        for (int64_t i = b; i < e; i++) {
+            if (use_sobol) {
+                uint32_t idx = offset + (uint32_t)i;
+                if (i > b) {
+                    int k = __builtin_ctz(idx);
+                    for (int dd = 0; dd < D; dd++) x[dd] ^= L[dd * 33 + k];
+                }
+                for (int dd = 0; dd < D; dd++) z[dd] = orc_ppnd16((double)orc_u_of(x[dd], flags));
+            } else {
+                orc_philox_normals(seed, salt_base + (uint32_t)r, (uint64_t)offset + (uint64_t)i, D, z);
+            }
+            double y = orc_is_payoff(m, p, n_steps, z_star, z);
+            s1 += y; s2 += y * y;
+        }
+        part[task * 2] = s1; part[task * 2 + 1] = s2;
+        free(x); free(z);
+    }
+    for (int r = 0; r < R; r++) {
+        double a = 0, b2 = 0;
+        for (int c = 0; c < nch; c++) { a += part[((size_t)r * nch + c) * 2]; b2 += part[((size_t)r * nch + c) * 2 + 1]; }
+        sums[r * 2] = a; sums[r * 2 + 1] = b2;
+    }
+    free(part); free(Lv);
+    return 0;
+}
+
 /* run_qmc_cuda's doubling loop (methods_cuda.cu:1624-1668) with an explicit start size. */
 int orc_run_qmc(const mcq_model* m, const mcq_payoff* p, double eps, int n_steps,
                 const orc_noise* nz, int R, int max_doublings, int64_t N0, uint32_t salt_base,

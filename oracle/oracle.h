@@ -99,6 +99,12 @@ int orc_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M,
 int orc_basket_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, uint32_t salt_base,
                           int R, uint32_t offset, int64_t N, int flags, int n_threads, double* sums);
 /* sums[2] over Philox paths first_path .. first_path + n_paths - 1 of (seed, stream) */
+/* kernel_is_gbm (methods_cuda.cu:685-707) in FP64: per-replica IS sums over scrambled Sobol or
+   Philox normals; z_star is the per-step drift shift. */
+double orc_is_payoff(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star, const double* z);
+int orc_is_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star, int use_sobol,
+                uint32_t seed, uint32_t salt_base, int R, uint32_t offset, int64_t N, int flags,
+                int n_threads, double* sums);
 int orc_mc_sums(const mcq_model* m, const mcq_payoff* p, int n_steps, uint32_t seed,
                 uint32_t stream, int64_t first_path, int64_t n_paths, int n_threads,
                 double* sums);

@@ -207,6 +207,17 @@ def basket_level_sums(m, p, n_fine, M, salt_base=42, R=1, offset=0, N=1024, flag
     return out
 
 
+def is_sums(m, p, n_steps, z_star, use_sobol=True, seed=42, salt_base=42, R=1, offset=0, N=1024, flags=0,
+            threads=0):
+    """kernel_is_gbm in FP64 (z_star: the per-step shift); sums[R][2] = {sum Y, sum Y^2}."""
+    out = np.zeros((R, 2))
+    rc = lib().orc_is_sums(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_double(z_star), C.c_int(int(use_sobol)),
+                           C.c_uint32(seed), C.c_uint32(salt_base), C.c_int(R), C.c_uint32(offset), C.c_int64(N),
+                           C.c_int(flags), C.c_int(threads), out.ctypes.data_as(_pd))
+    assert rc == 0, rc
+    return out
+
+
 def mc_sums(m, p, n_steps, seed, stream, first_path, n_paths, threads=0):
     out = np.zeros(2)
     lib().orc_mc_sums(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_uint32(seed), C.c_uint32(stream),
@@ -236,3 +247,78 @@ def bb_apply(N, T_, z):
                        ri.ctypes.data_as(_P(C.c_int)), wl.ctypes.data_as(_pd), wr.ctypes.data_as(_pd),
                        sd.ctypes.data_as(_pd), z.ctypes.data_as(_pd), dW.ctypes.data_as(_pd))
     return dW
+
+
+def run_mlqmc(m, p, eps, M=2, max_L=8, n0=1, pilot_n=1000, R=16, salt_base=42, flags=0, threads=0,
+              basket=False, max_iter=50):
+    """MLQMC adaptive driver in FP64 on the oracle's coupled level sums: the arithmetic of
+    run_mlqmc_cuda (methods_cuda.cu:1680-2016) — pilots on levels 0..2, N_opt =
+    ceil(2 / (R eps^2) sqrt(sig2_l / C_l) sum_k sqrt(sig2_k C_k)) with N_opt >= 100, merge of
+    the extra samples, bias test max(|E_L|, |E_{L-1}|) / (M - 1) < eps / sqrt(2), a new level
+    from its pilot, 50 iterations at most.  Level l uses salts salt_base + l R + r (Sobol while
+    its n0 M^l x factors dimensions fit the 20000-dimension table, Philox key salt_base and
+    stream salt_base + l R + r beyond).  basket=True runs the correlated GBM basket pair
+    (orc_basket_level_sums) and also returns the per-asset pathwise deltas."""
+    nd = m.n_assets if basket else (2 if m.kind == T.HESTON else 1)
+    E = [0.0] * (max_L + 1)
+    sig2 = [0.0] * (max_L + 1)
+    Nl = [0] * (max_L + 1)
+    off = [0] * (max_L + 1)
+    dl = [np.zeros(nd) for _ in range(max_L + 1)]
+    ps = [0.0]
+
+    def nfine(l):
+        return n0 * M ** l
+
+    def level(l, n):
+        nf = nfine(l)
+        salt = salt_base + l * R
+        if basket:
+            s = basket_level_sums(m, p, nf, M if l else 0, salt_base=salt, R=R, offset=off[l], N=n, flags=flags,
+                                  threads=threads)
+        else:
+            sob = nf * nd <= 20000
+            s = level_sums(m, p, nf, M if l else 0, None, use_sobol=sob, seed=salt_base, salt_base=salt, R=R,
+                           offset=off[l], N=n, flags=flags, threads=threads)
+        off[l] += n
+        ps[0] += R * n * (nf + (nf // M if l else 0))
+        rm = s[:, 0] / n
+        mm = rm.mean()
+        v = ((rm - mm) ** 2).sum() / (R - 1) if R > 1 else 0.0
+        d = (s[:, 4:4 + nd] / n).mean(axis=0) if basket else np.zeros(nd)
+        return mm, v, d
+
+    def absorb(l, n, res):
+        mm, v, d = res
+        if Nl[l] == 0:
+            E[l], sig2[l], dl[l] = mm, v * n, d
+        else:
+            wo, wn = float(Nl[l]), float(n)
+            E[l] = (E[l] * wo + mm * wn) / (wo + wn)
+            sig2[l] = (sig2[l] * wo + v * wn * wn) / (wo + wn)
+            dl[l] = (dl[l] * wo + d * wn) / (wo + wn)
+        Nl[l] += n
+
+    L = 2
+    for l in range(L + 1):
+        absorb(l, pilot_n, level(l, pilot_n))
+    converged, it = False, 0
+    while not converged and L <= max_L and it < max_iter:
+        it += 1
+        st = sum(np.sqrt(sig2[l] * M ** l) for l in range(L + 1))
+        for l in range(L + 1):
+            nopt = max(int(np.ceil(2.0 / (R * eps * eps) * np.sqrt(sig2[l] / M ** l) * st)), 100)
+            if nopt > Nl[l]:
+                absorb(l, nopt - Nl[l], level(l, nopt - Nl[l]))
+        bias = abs(E[L]) / max(M - 1, 1)
+        if L >= 1:
+            bias = max(bias, abs(E[L - 1]) * M / max(M * (M - 1), 1))
+        converged = bias < eps / np.sqrt(2.0)
+        if not converged and L < max_L:
+            L += 1
+            absorb(L, pilot_n, level(L, pilot_n))
+    price = sum(E[:L + 1])
+    se = float(np.sqrt(sum(sig2[l] / (Nl[l] * R) for l in range(L + 1))))
+    return {"price": price, "std_error": se, "levels": L + 1, "converged": converged,
+            "n_samples": int(sum(Nl[:L + 1]) * R), "path_steps": ps[0],
+            "delta": sum(dl[:L + 1]) if basket else None}

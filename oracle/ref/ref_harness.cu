@@ -204,6 +204,81 @@ extern "C" int mcqref_qmc_pass(const mcq_model* m, const mcq_payoff* p, int n_st
     HARNESS_END
 }
 
+// kernel_mlmc (methods_cuda.cu:445-518) as run_mlqmc_cuda's launch_level runs one level in raw
+// mode (:1849-1919), with the point count pinned: per replica, scrambled Sobol normals for salt
+// salt0 + r from point `offset`, kernel_scale by sqrt(h_fine) (not for Heston, which scales
+// inside), then the level kernel.  level0 != 0: no coarse path (N_coarse = 0, as level 0).
+// sums[4r .. 4r + 3] = {sum dY, sum dY^2, sum Yf, sum Yf^2}.
+extern "C" int mcqref_level_pass(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, int level0,
+                                 unsigned salt0, int R, unsigned offset, long long N, double* sums) {
+    HARNESS_TRY
+    ModelVariant mv = to_ref_model(*m);
+    PayoffVariant pv = to_ref_payoff(*p);
+    const ModelKind mk = model_kind(mv);
+    const int pidx = payoff_idx(pv);
+    if (mk == ModelKind::MultiDupire) throw std::runtime_error("the reference has no multi-asset level kernel");
+    KernelParams kp = make_params(mv, pv, 1);   // as run_mlqmc_cuda, :1720-1722
+    kp.M_refine = M;
+    CUDA_CHECK(cudaMemcpyToSymbol(c_p, &kp, sizeof(kp)));
+    const double T = model_T(mv);
+    const int N_fine = n_fine, N_coarse = level0 ? 0 : n_fine / M;
+    const float h_fine = (float)(T / N_fine), h_coarse = (float)(T / std::max(N_coarse, 1));
+    const float sqrt_hf = sqrtf(h_fine);
+    const long long D = (long long)N_fine * model_noise_dim(mv);
+    const long long gen_count = (D * N + 1) & ~1LL;
+    float* d_Z = nullptr;
+    double* d_sums = nullptr;
+    CUDA_CHECK(cudaMalloc(&d_Z, (D * N + 2) * sizeof(float)));
+    CUDA_CHECK(cudaMalloc(&d_sums, 4 * sizeof(double)));
+    for (int r = 0; r < R; r++) {
+        CUDA_CHECK(cudaMemset(d_sums, 0, 4 * sizeof(double)));
+        gen_scrambled_sobol_normal_replica(d_Z, D, N, offset, salt0 + (unsigned)r);
+        if (mk != ModelKind::Heston)
+            kernel_scale<<<(int)((gen_count + BLOCK_SIZE - 1) / BLOCK_SIZE), BLOCK_SIZE>>>(d_Z, sqrt_hf, gen_count);
+        MLMC_TABLE[(int)mk][pidx]<<<(int)((N + BLOCK_SIZE - 1) / BLOCK_SIZE), BLOCK_SIZE>>>(
+            d_Z, d_sums, (int)N, N_fine, N_coarse, M, h_fine, h_coarse, sqrt_hf);
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaDeviceSynchronize());
+        CUDA_CHECK(cudaMemcpy(sums + 4 * r, d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    cudaFree(d_Z); cudaFree(d_sums);
+    HARNESS_END
+}
+
+// kernel_is_gbm (methods_cuda.cu:685-707) with the parameters run_is_cuda sets (:2288-2298) and
+// scrambled Sobol normals (salt salt0 + r, from point `offset`) in place of its XORWOW stream;
+// z_star_step is the per-step shift.  sums[2r], sums[2r + 1] = {sum Y, sum Y^2}.
+extern "C" int mcqref_is_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_star_step,
+                              unsigned salt0, int R, unsigned offset, long long N, double* sums) {
+    HARNESS_TRY
+    if (m->kind != MCQ_MODEL_GBM || p->kind != MCQ_PAYOFF_EUROPEAN) throw std::runtime_error("IS: GBM European");
+    KernelParams kp{};
+    kp.S0 = (float)m->S0; kp.mu = (float)m->mu; kp.sigma = (float)m->sigma; kp.T = (float)m->T;
+    kp.K = (float)p->K; kp.r = (float)p->r;
+    kp.discount = (float)std::exp(-p->r * p->T);
+    kp.payoff_kind = PayoffKind::European;
+    kp.z_star = (float)z_star_step;
+    kp.h = kp.T / n_steps;
+    CUDA_CHECK(cudaMemcpyToSymbol(c_p, &kp, sizeof(kp)));
+    float* d_Z = nullptr;
+    double* d_sums = nullptr;
+    CUDA_CHECK(cudaMalloc(&d_Z, ((long long)n_steps * N + 2) * sizeof(float)));
+    CUDA_CHECK(cudaMalloc(&d_sums, 4 * sizeof(double)));
+    for (int r = 0; r < R; r++) {
+        CUDA_CHECK(cudaMemset(d_sums, 0, 4 * sizeof(double)));
+        gen_scrambled_sobol_normal_replica(d_Z, n_steps, N, offset, salt0 + (unsigned)r);
+        kernel_is_gbm<<<(int)((N + BLOCK_SIZE - 1) / BLOCK_SIZE), BLOCK_SIZE>>>(d_Z, d_sums, (int)N, n_steps);
+        CUDA_CHECK(cudaGetLastError());
+        CUDA_CHECK(cudaDeviceSynchronize());
+        double hs[4];
+        CUDA_CHECK(cudaMemcpy(hs, d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+        sums[2 * r] = hs[0];
+        sums[2 * r + 1] = hs[1];
+    }
+    cudaFree(d_Z); cudaFree(d_sums);
+    HARNESS_END
+}
+
 // The reference's adaptive drivers, unmodified, for statistical comparison.
 extern "C" int mcqref_run_mlqmc(const mcq_model* m, const mcq_payoff* p, double eps, int M, int max_L,
                                 int pilot_n, int R, double* out4) {

@@ -35,3 +35,36 @@ def cases(T):
         ("basket4_32", T.multi_dupire(100 * rng.uniform(0.8, 1.2, n), L), T.basket(100.0, 0.05, 1.0, n), 32, T.RAW,
          42, 2, 0, 4096),
     ]
+
+
+def level_cases(T):
+    """Coupled level passes of the reference's kernel_mlmc (methods_cuda.cu:445-518), n0 = 1 as the
+    reference (N_fine = M^l): (name, model, payoff, level, M, salt0, R, offset, N).  The recorded
+    salt may be moved by make_ref_golden.py off a window with a u = 1 point."""
+    gbm, hes = T.gbm(100.0, 0.05, 0.2, 1.0), T.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)
+    dup = T.dupire(100.0, 0.05, 0.2, 0.5, 0.7, 1.0)
+    out = []
+    for lv in range(4):
+        out.append((f"lvl_gbm_eur_M4_l{lv}", gbm, T.european(100.0, 0.05, 1.0), lv, 4, 500 + lv, 2, 0, 4096))
+        out.append((f"lvl_heston_eur_M4_l{lv}", hes, T.european(100.0, 0.02, 1.0), lv, 4, 520 + lv, 2, 0, 4096))
+        out.append((f"lvl_dupire_eur_M2_l{lv}", dup, T.european(100.0, 0.05, 1.0), lv, 2, 540 + lv, 2, 0, 4096))
+    for lv in (1, 3):
+        out.append((f"lvl_gbm_asian_M2_l{lv}", gbm, T.asian(100.0), lv, 2, 560 + lv, 2, 64, 4096))
+        out.append((f"lvl_gbm_lookback_M4_l{lv}", gbm, T.lookback(0.2), lv, 4, 580 + lv, 2, 0, 4096))
+        # the reference's Heston level kernel skips the running update (trap of :464-490): the
+        # engine matches it under MCQ_FLAG_COMPAT_HESTON_MLMC
+        out.append((f"lvl_heston_lookback_M4_l{lv}", hes, T.lookback(0.2), lv, 4, 600 + lv, 2, 0, 4096))
+    out.append(("lvl_gbm_upout_M4_l2", gbm, T.barrier_up_out(100.0, 125.0, 0.2, 0.05, 1.0), 2, 4, 620, 2, 0, 4096))
+    return out
+
+
+def is_cases(T):
+    """kernel_is_gbm (methods_cuda.cu:685-707) on scrambled Sobol normals:
+    (name, model, payoff, n_steps, z_star (whole path; the kernel takes z_star / sqrt(n_steps)),
+    salt0, R, offset, N)."""
+    gbm = T.gbm(100.0, 0.05, 0.2, 1.0)
+    return [
+        ("is_atm_64", gbm, T.european(100.0, 0.05, 1.0), 64, 0.5, 700, 2, 0, 4096),
+        ("is_otm180_100", gbm, T.european(180.0, 0.05, 1.0), 100, 3.0, 710, 2, 0, 4096),
+        ("is_otm180_100_off", gbm, T.european(180.0, 0.05, 1.0), 100, 3.0, 720, 2, 8192, 4096),
+    ]

@@ -10,6 +10,15 @@ its sources by `make -C oracle ref`) and records
   * results of its adaptive run_mc / run_mlmc / run_mlqmc drivers (statistical checks),
   * device time of the reference's pass for the RQMC Asian workload (the plain comparator).
 Usage: python tests/golden/make_ref_golden.py [out.npz]
+
+python tests/golden/make_ref_golden.py --levels writes ref_golden_levels.npz (+ .json) instead:
+  * per-replica {sum dY, sum dY^2, sum Yf, sum Yf^2} of the reference's coupled level kernel
+    kernel_mlmc (:445-518) as run_mlqmc_cuda runs a raw level (:1849-1919), GBM / Heston /
+    Dupire, M = 2 and 4, levels 0-3 (golden_cases.level_cases),
+  * per-replica {sum Y, sum Y^2} of its importance-sampling kernel kernel_is_gbm (:685-707) on
+    scrambled Sobol normals (golden_cases.is_cases).
+A case whose window holds a point with u = 1 (scrambled word >= 0xFFFFFF80) moves to the next
+salt (+ 1000) until it has none; the JSON records the salt used.
 """
 import ctypes as C
 import json
@@ -29,7 +38,7 @@ T = orc.T
 REF = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libmcqref.so"))
 REF.mcqref_last_error.restype = C.c_char_p
 
-from golden_cases import SALTS, OFFSETS, DIMS, cases as _cases  # noqa: E402
+from golden_cases import SALTS, OFFSETS, DIMS, cases as _cases, level_cases, is_cases  # noqa: E402
 
 
 def ok(rc):
@@ -121,5 +130,46 @@ def main(out):
         json.dump(meta, f, indent=1)
 
 
+def ref_level(m, p, level, M, salt0, R, off, N):
+    sums = np.zeros(4 * R)
+    n_fine = M ** level
+    ok(REF.mcqref_level_pass(C.byref(m), C.byref(p), C.c_int(n_fine), C.c_int(M), C.c_int(int(level == 0)),
+                             C.c_uint(salt0), C.c_int(R), C.c_uint(off), C.c_longlong(N),
+                             sums.ctypes.data_as(C.POINTER(C.c_double))))
+    return sums.reshape(R, 4)
+
+
+def ref_is(m, p, n_steps, z_step, salt0, R, off, N):
+    sums = np.zeros(2 * R)
+    ok(REF.mcqref_is_pass(C.byref(m), C.byref(p), C.c_int(n_steps), C.c_double(z_step), C.c_uint(salt0),
+                          C.c_int(R), C.c_uint(off), C.c_longlong(N), sums.ctypes.data_as(C.POINTER(C.c_double))))
+    return sums.reshape(R, 2)
+
+
+def main_levels(out):
+    g, meta = {}, {"levels": [], "is": []}
+    for name, m, p, level, M, salt0, R, off, N in level_cases(T):
+        D = M ** level * T.noise_dim(m)
+        while top_edge_hits(salt0, R, D, off, N):
+            salt0 += 1000
+        g[name] = ref_level(m, p, level, M, salt0, R, off, N)
+        meta["levels"].append(dict(name=name, level=level, M=M, salt0=salt0, R=R, offset=off, N=N))
+        print(name, salt0, g[name][:, 0] / N, g[name][:, 2] / N, flush=True)
+    for name, m, p, n_steps, z_star, salt0, R, off, N in is_cases(T):
+        while top_edge_hits(salt0, R, n_steps, off, N):
+            salt0 += 1000
+        z_step = z_star / np.sqrt(n_steps)
+        g[name] = ref_is(m, p, n_steps, z_step, salt0, R, off, N)
+        meta["is"].append(dict(name=name, n_steps=n_steps, z_star=z_star, z_step=z_step, salt0=salt0, R=R,
+                               offset=off, N=N))
+        print(name, salt0, g[name][:, 0] / N, flush=True)
+    np.savez_compressed(out, **g)
+    with open(os.path.splitext(out)[0] + ".json", "w") as f:
+        json.dump(meta, f, indent=1)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "ref_golden.npz"))
+    if len(sys.argv) > 1 and sys.argv[1] == "--levels":
+        main_levels(os.path.join(HERE, "ref_golden_levels.npz"))
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "ref_golden.npz"))

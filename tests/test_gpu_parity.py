@@ -256,3 +256,22 @@ def test_heston_compat_u_inf_matches_reference(gpu, orc, parity, pay):
     assert same(gl[0, 2], ol[0, 2]) and same(gl[0, 0], ol[0, 0]), (dim, gl, ol)
     g0 = gpu.qmc_pass(m, p, 32, salt_base=42, R=1, offset=off, n_points=N)
     assert np.isfinite(g0[0, 0]) and abs(g0[0, 0] / N - o0[0, 0] / N) < tol(pay, N, o0[0, 0] / N)
+
+
+@pytest.mark.parametrize("use_sobol", [True, False])
+@pytest.mark.parametrize("K,z_star,n_steps", [(100.0, 0.5, 64), (180.0, 3.0, 100), (140.0, 1.5, 37)])
+def test_is_pass_vs_oracle(gpu, orc, use_sobol, K, z_star, n_steps):
+    """The importance-sampling pass (IsC; kernel_is_gbm, methods_cuda.cu:685-707) path by path in the
+    FP64 oracle on the same normals: drift-shifted Euler path, likelihood ratio, weighted payoff.
+    Per-replica means and second moments to FP32 rounding."""
+    m, p = gpu.gbm(100.0, 0.05, 0.2, 1.0), gpu.european(K, 0.05, 1.0)
+    zs = z_star / np.sqrt(n_steps)
+    R, N = 3, 2000
+    g = gpu.is_pass(m, p, n_steps, zs, use_sobol=use_sobol, seed=9, salt_base=31, R=R, offset=17, n_points=N)
+    o = orc.is_sums(m, p, n_steps, zs, use_sobol=use_sobol, seed=9, salt_base=31, R=R, offset=17, N=N)
+    for r in range(R):
+        assert abs(g[r, 0] / N - o[r, 0] / N) < 2e-4 * (1 + abs(o[r, 0] / N)), (r, g[r], o[r])
+        assert abs(g[r, 1] - o[r, 1]) < 1e-3 * (1 + abs(o[r, 1])), (r, g[r], o[r])
+    # the shift and the likelihood ratio are applied: the sums differ from those of z* = 0
+    g0 = gpu.is_pass(m, p, n_steps, 0.0, use_sobol=use_sobol, seed=9, salt_base=31, R=R, offset=17, n_points=N)
+    assert np.abs(g0[:, 0] - g[:, 0]).max() > 1e-3 * np.abs(g[:, 0]).max()
