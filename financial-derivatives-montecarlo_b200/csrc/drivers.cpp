@@ -173,9 +173,10 @@ void run_qmc(const mcq_model& m, const mcq_payoff& p, double eps, int n_steps,
 void run_mlmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_mlmc_cfg& cfg,
               mcq_result& out) {
     check_model_payoff(m, p);
-    MCQ_REQUIRE(m.kind != MCQ_MODEL_MULTI_DUPIRE, MCQ_ERR_UNSUPPORTED,
-                "run_mlmc: the Dupire basket has no coupled path (as methods_cuda.cu:1318-1320); the "
-                "correlated GBM basket does");
+    // the reference refuses baskets here (methods_cuda.cu:1318-1320); the engine couples the
+    // correlated GBM and Dupire baskets of up to kMaxBasket assets (BasketLevelC)
+    MCQ_REQUIRE((m.kind != MCQ_MODEL_MULTI_DUPIRE && m.kind != MCQ_MODEL_BASKET_GBM) || m.n_assets <= kMaxBasket,
+                MCQ_ERR_UNSUPPORTED, "run_mlmc: coupled baskets take at most 16 assets");
     MCQ_REQUIRE(eps > 0 && cfg.M >= 2 && cfg.max_L >= 2 && cfg.pilot_n >= 1 && cfg.n0_steps >= 1,
                 MCQ_ERR_INVALID, "run_mlmc: bad eps / M / max_L / pilot_n / n0_steps");
     auto t0 = Clock::now();
@@ -288,9 +289,10 @@ void run_mlqmc(const mcq_model& m, const mcq_payoff& p, double eps, const mcq_ml
                const mcq_qmc_cfg& qc, int noise, const std::vector<const Handle*>& bb_list,
                const std::vector<const Handle*>& pca_list, mcq_result& out) {
     check_model_payoff(m, p);
-    MCQ_REQUIRE(m.kind != MCQ_MODEL_MULTI_DUPIRE, MCQ_ERR_UNSUPPORTED,
-                "run_mlqmc: the Dupire basket has no coupled path (as methods_cuda.cu:1695-1697); the "
-                "correlated GBM basket does");
+    // the reference refuses baskets here (methods_cuda.cu:1695-1697); the engine couples the
+    // correlated GBM and Dupire baskets of up to kMaxBasket assets (BasketLevelC)
+    MCQ_REQUIRE((m.kind != MCQ_MODEL_MULTI_DUPIRE && m.kind != MCQ_MODEL_BASKET_GBM) || m.n_assets <= kMaxBasket,
+                MCQ_ERR_UNSUPPORTED, "run_mlqmc: coupled baskets take at most 16 assets");
     MCQ_REQUIRE(noise == MCQ_NOISE_RAW || noise_dim(m) == 1, MCQ_ERR_UNSUPPORTED,
                 "run_mlqmc: Brownian bridge / PCA only for one-factor models (:1702-1704)");
     MCQ_REQUIRE(eps > 0 && ml.M >= 2 && ml.max_L >= 2 && ml.pilot_n >= 1 && ml.n0_steps >= 1 && qc.R >= 1,

@@ -140,7 +140,7 @@ int noise_dim(const mcq_model& m) {   // model_noise_dim, models.hpp:78-87
 }
 
 int nstat_of(int est, int model) {
-    if (est == EST_COUPLED && model == MCQ_MODEL_BASKET_GBM) return 4 + kMaxBasket;
+    if (est == EST_COUPLED && (model == MCQ_MODEL_BASKET_GBM || model == MCQ_MODEL_MULTI_DUPIRE)) return 4 + kMaxBasket;
     return nstat_of(est);
 }
 
@@ -265,9 +265,14 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
         if (m.kind == MCQ_MODEL_BASKET_GBM)
             MCQ_REQUIRE(m.sigma_vec != nullptr, MCQ_ERR_INVALID, "basket needs sigma_vec");
         std::vector<float> pk((size_t)3 * n + (size_t)n * n, 0.f);
+        // the second block: per-asset sigma for the GBM basket; for the Dupire basket the inverse
+        // of the S0 that scales the asset's local volatility (asset 0's, as the reference, or
+        // its own under MCQ_FLAG_BASKET_OWN_S0)
+        const bool own = (a.flags & MCQ_FLAG_BASKET_OWN_S0) != 0;
         for (int i = 0; i < n; i++) {
             pk[i] = (float)m.S0_vec[i];
-            pk[n + i] = m.sigma_vec ? (float)m.sigma_vec[i] : 0.f;
+            if (m.kind == MCQ_MODEL_MULTI_DUPIRE) pk[n + i] = 1.0f / (float)m.S0_vec[own ? i : 0];
+            else pk[n + i] = m.sigma_vec ? (float)m.sigma_vec[i] : 0.f;
             pk[2 * n + i] = m.weights ? (float)m.weights[i] : 1.0f / n;
         }
         const bool unc = m.uncorrelated || !m.L;
@@ -479,7 +484,8 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     }
 
     const int skel = (a.noise == NOISE_BB && D > 32) ? ((D >> 5) + 1) * 32 : 0;
-    const int accf = (!a.dump && a.est == EST_COUPLED && k.model == MOD_BASKET) ? ((2 * nst + 3) & ~3) : 0;
+    const int accf = (!a.dump && a.est == EST_COUPLED && (k.model == MOD_BASKET || k.model == MOD_MULTI))
+                         ? ((2 * nst + 3) & ~3) : 0;
     const size_t smem = assist ? (size_t)kAssistTeams * kAssistTeamBytes
                                : (size_t)kWarpsPerBlock * (1024 + skel + accf) * sizeof(float);
     KernelInfo& ki = kernel_info(fn, smem);

@@ -14,9 +14,15 @@ static const void* misc_gen(int noise, int est, int model, int nb, bool dump) {
     if (est == EST_CV_DUPIRE) return (const void*)&k_pass<GEN, NOISE_RAW, CvDupireC>;
     if (est == EST_IS) return (const void*)&k_pass<GEN, NOISE_RAW, IsC>;
     if (est == EST_COUPLED && model == MOD_BASKET) {
-        if (nb <= 4) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<4>>;
-        if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<8>, 2>;
-        if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<16>, 1>;
+        if (nb <= 4) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<MOD_BASKET, 4>>;
+        if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<MOD_BASKET, 8>, 2>;
+        if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<MOD_BASKET, 16>, 1>;
+        return nullptr;
+    }
+    if (est == EST_COUPLED && model == MOD_MULTI) {
+        if (nb <= 4) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<MOD_MULTI, 4>>;
+        if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<MOD_MULTI, 8>, 2>;
+        if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketLevelC<MOD_MULTI, 16>, 1>;
         return nullptr;
     }
     if (model == MOD_MULTI) {

@@ -23,6 +23,8 @@ enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3,
 
 // Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
 constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
+// MCQ_FLAG_BASKET_OWN_S0 as the kernels test it in KParams::flags.
+constexpr int MCQ_FLAG_OWN_S0_CODE = 16;
 enum ModelK : int { MOD_GBM = 0, MOD_HESTON = 1, MOD_DUPIRE = 2, MOD_MULTI = 3, MOD_LVGRID = 4, MOD_BASKET = 5 };
 enum PayK : int { PAY_EUR = 0, PAY_ASIAN = 1, PAY_GEOM = 2, PAY_LOOKBACK = 3, PAY_UPOUT = 4, PAY_BASKET = 5, PAY_DOWNOUT = 6 };
 enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE = 3, EST_IS = 4 };

@@ -520,8 +520,10 @@ struct IsC {
 
 // Multi-asset basket (kernel_multi_dupire, methods_cuda.cu:525-551, with the Cholesky product
 // of correlate_multi_dupire :1122-1148 done in registers): dims of step k are k*n + a.
-// MOD_MULTI: parametric Dupire per asset with the reference's asset-0 S0 inside sigma_loc
-// (:542, :289); MOD_BASKET: GBM per asset with its own sigma, weighted basket.
+// MOD_MULTI: parametric Dupire per asset; sigma_loc's S0 scale is read per asset from the second
+// block of p.bsk (1 / S0 of asset 0 for every asset, the reference's c_p.S0 (:542, :289), or the
+// asset's own under MCQ_FLAG_BASKET_OWN_S0); MOD_BASKET: GBM per asset with its own sigma,
+// weighted basket.
 template <int MOD, int NB>
 struct BasketC {
     static constexpr int NST = 2;
@@ -555,7 +557,8 @@ struct BasketC {
             for (int a = 0; a < NB; a++) {
                 if (a < n) {
                     if constexpr (MOD == MOD_MULTI) {
-                        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * p.inv_S0), -p.alpha * t * kLog2e));
+                        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * __ldg(p.bsk + n + a)),
+                                                               -p.alpha * t * kLog2e));
                         S[a] = fmaf(S[a], fmaf(sl, dw[a], muh), S[a]);
                     } else {
                         S[a] = fmaf(S[a], fmaf(__ldg(p.bsk + n + a), dw[a], muh), S[a]);
@@ -614,18 +617,26 @@ struct DumpC {
     __device__ __forceinline__ void finish(const KParams&, float (&y)[NST]) { y[0] = 0.f; }
 };
 
-// Coupled fine / coarse correlated GBM basket for MLMC / MLQMC levels (the reference refuses
+// Coupled fine / coarse correlated basket for MLMC / MLQMC levels (the reference refuses
 // baskets there, methods_cuda.cu:1318-1320, :1695-1697), with the pathwise delta per asset.
-// Euler GBM is linear in S0_a, so dS_a(T)/dS0_a = S_a(T)/S0_a and
-// delta_a = disc 1{B > K} w_a S_a(T) / S0_a on each of the fine and coarse paths.
+// MOD_BASKET: GBM per asset with its own sigma and a weighted basket.  Euler GBM is linear in
+// S0_a, so dS_a(T)/dS0_a = S_a(T)/S0_a and delta_a = disc 1{B > K} w_a S_a(T) / S0_a on each of
+// the fine and coarse paths.
+// MOD_MULTI: the reference's Dupire basket (parametric local vol per asset, equally weighted
+// mean, kernel_multi_dupire :525-551) stepped as kernel_mlmc steps a one-asset Dupire path
+// (:471-497): fine steps at t = k h, coarse steps at t = k_c h_c on the summed increments.  Under
+// MCQ_FLAG_BASKET_OWN_S0 each asset's volatility is scaled by its own S0, the path is then
+// homogeneous of degree one in (S0_a, S_a) and the same delta formula is the total derivative
+// dP/dS0_a (the scale inside sigma_loc moving with S0_a, as the one-asset Dupire adjoint); with
+// the reference's asset-0 scale it is not, and the deltas are left at 0.
 // Statistics: {dY, dY^2, Yf, Yf^2, d delta_0 .. d delta_15}.
-template <int NB>
+template <int MOD, int NB>
 struct BasketLevelC {
     static constexpr int NST = 4 + kMaxBasket;
     static constexpr bool WARP_ACC = true;
     float Sf[NB], Sc[NB], dw[NB], acc[NB];
     float muh_f, muh_c;
-    int f, m;
+    int f, m, k, kc;
     __device__ __forceinline__ void bind(int, uint64_t) {}
     __device__ __forceinline__ void flush() {}
     __device__ __forceinline__ void init(const KParams& p) {
@@ -637,7 +648,14 @@ struct BasketLevelC {
         }
         muh_f = p.mu * p.h;
         muh_c = p.mu * p.hc;
-        f = 0; m = 0;
+        f = 0; m = 0; k = 0; kc = 0;
+    }
+    // sigma_loc(S, t) S-scale: the per-asset inverse reference S0 (second block of p.bsk)
+    __device__ __forceinline__ float vol(const KParams& p, int n, int a, float S, float t) const {
+        if constexpr (MOD == MOD_MULTI)
+            return p.sigma0 * exp2f(fmaf(p.bm1, log2f(S * __ldg(p.bsk + n + a)), -p.alpha * t * kLog2e));
+        else
+            return __ldg(p.bsk + n + a);
     }
     __device__ __forceinline__ void feed(const KParams& p, float z) {
         const int n = p.n_assets;
@@ -653,21 +671,22 @@ struct BasketLevelC {
         }
         if (++f == n) {
             const bool coarse = (++m == p.M);
+            const float t = (float)k * p.h, tc = (float)kc * p.hc;
 #pragma unroll
             for (int a = 0; a < NB; a++) {
                 if (a < n) {
-                    const float sg = __ldg(p.bsk + n + a);
-                    Sf[a] = fmaf(Sf[a], fmaf(sg, dw[a], muh_f), Sf[a]);
+                    Sf[a] = fmaf(Sf[a], fmaf(vol(p, n, a, Sf[a], t), dw[a], muh_f), Sf[a]);
                     acc[a] += dw[a];
                     if (coarse) {
-                        Sc[a] = fmaf(Sc[a], fmaf(sg, acc[a], muh_c), Sc[a]);
+                        Sc[a] = fmaf(Sc[a], fmaf(vol(p, n, a, Sc[a], tc), acc[a], muh_c), Sc[a]);
                         acc[a] = 0.f;
                     }
                 }
                 dw[a] = 0.f;
             }
-            if (coarse) m = 0;
+            if (coarse) { m = 0; kc++; }
             f = 0;
+            k++;
         }
     }
     __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
@@ -679,23 +698,32 @@ struct BasketLevelC {
     __device__ __forceinline__ void finish(const KParams& p, float (&y)[NST]) {
         const int n = p.n_assets;
         float Bf = 0.f, Bc = 0.f;
+        if constexpr (MOD == MOD_MULTI) {   // equally weighted mean, as kernel_multi_dupire
 #pragma unroll
-        for (int a = 0; a < NB; a++)
-            if (a < n) {
-                const float w = __ldg(p.bsk + 2 * n + a);
-                Bf = fmaf(w, Sf[a], Bf);
-                Bc = fmaf(w, Sc[a], Bc);
-            }
+            for (int a = 0; a < NB; a++)
+                if (a < n) { Bf += Sf[a]; Bc += Sc[a]; }
+            Bf = Bf / (float)n;
+            Bc = Bc / (float)n;
+        } else {
+#pragma unroll
+            for (int a = 0; a < NB; a++)
+                if (a < n) {
+                    const float w = __ldg(p.bsk + 2 * n + a);
+                    Bf = fmaf(w, Sf[a], Bf);
+                    Bc = fmaf(w, Sc[a], Bc);
+                }
+        }
         const bool has_c = p.n_coarse > 0;
         const float yf = fmaxf(Bf - p.K, 0.f) * p.disc;
         const float yc = has_c ? fmaxf(Bc - p.K, 0.f) * p.disc : 0.f;
         const float dy = yf - yc;
         y[0] = dy; y[1] = dy * dy; y[2] = yf; y[3] = yf * yf;
+        const bool deltas = (MOD == MOD_BASKET) || (p.flags & MCQ_FLAG_OWN_S0_CODE);
         const float gf = (Bf > p.K) ? p.disc : 0.f, gc = (has_c && Bc > p.K) ? p.disc : 0.f;
 #pragma unroll
         for (int a = 0; a < kMaxBasket; a++) {
             float v = 0.f;
-            if (a < NB && a < n) {
+            if (a < NB && a < n && deltas) {
                 const float wa = __ldg(p.bsk + 2 * n + a) / __ldg(p.bsk + a);
                 v = wa * (gf * Sf[a] - gc * Sc[a]);
             }
@@ -737,7 +765,8 @@ struct BasketWideC {
 #pragma unroll 1
             for (int a = 0; a < n; a++) {
                 if constexpr (MOD == MOD_MULTI) {
-                    const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * p.inv_S0), -p.alpha * t * kLog2e));
+                    const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * __ldg(p.bsk + n + a)),
+                                                           -p.alpha * t * kLog2e));
                     S[a] = fmaf(S[a], fmaf(sl, dw[a], muh), S[a]);
                 } else {
                     S[a] = fmaf(S[a], fmaf(__ldg(p.bsk + n + a), dw[a], muh), S[a]);
@@ -1041,8 +1070,8 @@ __host__ __device__ constexpr bool noise_is_bb(int noise) { return noise == NOIS
 // allocation and scheduling, never in arithmetic, so they produce identical sums.
 template <class C>
 struct warp_acc_of { static constexpr bool value = false; };
-template <int NB>
-struct warp_acc_of<BasketLevelC<NB>> { static constexpr bool value = true; };
+template <int MOD, int NB>
+struct warp_acc_of<BasketLevelC<MOD, NB>> { static constexpr bool value = true; };
 
 template <int GEN, int NOISE, class C, int MINB = 0>
 __global__ void __launch_bounds__(kThreads, MINB ? MINB : (noise_is_bb(NOISE) ? 2 : kMinBlocks))

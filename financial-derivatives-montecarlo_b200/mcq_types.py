@@ -14,6 +14,7 @@ RAW, BB, PCA = range(3)
 FLAG_COMPAT_U_INF = 1
 FLAG_COMPAT_HESTON_MLMC = 2
 FLAG_HESTON_MILSTEIN = 8
+FLAG_BASKET_OWN_S0 = 16
 
 _pd = C.POINTER(C.c_double)
 

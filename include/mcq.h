@@ -69,6 +69,10 @@ extern "C" {
 #define MCQ_FLAG_HESTON_MILSTEIN     8  /* Heston variance step with the Milstein term
                                            xi^2/4 (dW2^2 - h) (Euler-Milstein, full truncation);
                                            default: the reference's Euler step (:276-284) */
+#define MCQ_FLAG_BASKET_OWN_S0      16  /* Dupire basket: scale each asset's local volatility
+                                           by its own S0, sigma0 e^{-alpha t} (S_a / S0_a)^(beta-1);
+                                           default: asset 0's S0 for every asset, as the
+                                           reference (c_p.S0 = S0[0], methods_cuda.cu:1046, :538-542) */
 
 /* ---------------------------------------------------------------- parameter structs */
 typedef struct mcq_model {

@@ -502,6 +502,7 @@ double orc_path_payoff_f(const mcq_model* m, const mcq_payoff* p, int n_steps,
         double* dwc = (double*)malloc(sizeof(double) * n);
         for (int a = 0; a < n; a++) Sa[a] = m->S0_vec ? m->S0_vec[a] : m->S0;
         double S0ref = m->S0_vec ? m->S0_vec[0] : m->S0;   /* c_p.S0 = S0[0], :1046 */
+        int own = (flags & MCQ_FLAG_BASKET_OWN_S0) != 0;   /* each asset's own S0 in sigma_loc */
         for (int k = 0; k < n_steps; k++) {
             for (int a = 0; a < n; a++) {
                 double acc = 0;
@@ -512,7 +513,8 @@ double orc_path_payoff_f(const mcq_model* m, const mcq_payoff* p, int n_steps,
             for (int a = 0; a < n; a++) {
                 double S = Sa[a];
                 if (m->kind == MCQ_MODEL_MULTI_DUPIRE) {
-                    double sl = m->sigma0 * exp(-m->alpha * (k * h)) * pow(S / S0ref, m->beta_d - 1.0);
+                    double s0 = own ? m->S0_vec[a] : S0ref;
+                    double sl = m->sigma0 * exp(-m->alpha * (k * h)) * pow(S / s0, m->beta_d - 1.0);
                     Sa[a] = S + m->mu * S * h + sl * S * dwc[a];
                 } else {
                     Sa[a] = S + m->mu * S * h + m->sigma_vec[a] * S * dwc[a];
@@ -743,7 +745,20 @@ int orc_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, int M,
  * M <= 0: level 0 (no coarse path).  Returns Yf; *yc = Yc; dd[a] = d(Yf - Yc)/dS0_a. */
 double orc_basket_level(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, const double* z,
                         double* yc, double* dd) {
+    return orc_basket_level_f(m, p, n_fine, M, z, yc, dd, 0);
+}
+
+/* The coupled basket pair for the correlated GBM basket (weighted, per-asset sigma) and the
+ * reference's Dupire basket (equally weighted mean, sigma_loc with asset 0's S0, or each asset's
+ * own under MCQ_FLAG_BASKET_OWN_S0), stepped as kernel_mlmc steps one Dupire path
+ * (methods_cuda.cu:471-497: fine steps at t = k h, coarse steps at t = k_c h_c on the summed
+ * increments).  dd[a] = w_a / S0_a (gf Sf_a - gc Sc_a): the pathwise dP/dS0_a of the GBM basket,
+ * and of the Dupire basket under MCQ_FLAG_BASKET_OWN_S0 (the path is then homogeneous in
+ * (S0_a, S_a)); 0 for the Dupire basket with the reference's asset-0 scale. */
+double orc_basket_level_f(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, const double* z,
+                          double* yc, double* dd, int flags) {
     int n = m->n_assets, coarse = M > 0, Mr = coarse ? M : 1;
+    int dup = m->kind == MCQ_MODEL_MULTI_DUPIRE, own = (flags & MCQ_FLAG_BASKET_OWN_S0) != 0;
     int n_coarse = coarse ? n_fine / Mr : 0;
     double hf = m->T / n_fine, hc = m->T / (n_coarse > 0 ? n_coarse : 1), sq = sqrt(hf);
     double *Sf = (double*)malloc(sizeof(double) * 4 * n), *Sc = Sf + n, *dw = Sf + 2 * n, *acc = Sf + 3 * n;
@@ -757,19 +772,28 @@ double orc_basket_level(const mcq_model* m, const mcq_payoff* p, int n_fine, int
             dw[a] = v;
         }
         for (int a = 0; a < n; a++) {
-            Sf[a] = Sf[a] + m->mu * Sf[a] * hf + m->sigma_vec[a] * Sf[a] * dw[a];
+            double vol = m->sigma_vec ? m->sigma_vec[a] : 0.0;
+            if (dup)
+                vol = m->sigma0 * exp(-m->alpha * (k * hf)) *
+                      pow(Sf[a] / m->S0_vec[own ? a : 0], m->beta_d - 1.0);
+            Sf[a] = Sf[a] + m->mu * Sf[a] * hf + vol * Sf[a] * dw[a];
             acc[a] += dw[a];
         }
         if (coarse && (k + 1) % Mr == 0) {
+            int kc = (k + 1) / Mr - 1;
             for (int a = 0; a < n; a++) {
-                Sc[a] = Sc[a] + m->mu * Sc[a] * hc + m->sigma_vec[a] * Sc[a] * acc[a];
+                double vol = m->sigma_vec ? m->sigma_vec[a] : 0.0;
+                if (dup)
+                    vol = m->sigma0 * exp(-m->alpha * (kc * hc)) *
+                          pow(Sc[a] / m->S0_vec[own ? a : 0], m->beta_d - 1.0);
+                Sc[a] = Sc[a] + m->mu * Sc[a] * hc + vol * Sc[a] * acc[a];
                 acc[a] = 0;
             }
         }
     }
     double Bf = 0, Bc = 0, disc = pay_discount(p);
     for (int a = 0; a < n; a++) {
-        double w = m->weights ? m->weights[a] : 1.0 / n;
+        double w = (m->weights && !dup) ? m->weights[a] : 1.0 / n;
         Bf += w * Sf[a];
         Bc += w * Sc[a];
     }
@@ -777,8 +801,8 @@ double orc_basket_level(const mcq_model* m, const mcq_payoff* p, int n_fine, int
     *yc = n_coarse > 0 ? fmax(Bc - p->K, 0.0) * disc : 0.0;
     double gf = Bf > p->K ? disc : 0.0, gc = (n_coarse > 0 && Bc > p->K) ? disc : 0.0;
     for (int a = 0; a < n; a++) {
-        double w = m->weights ? m->weights[a] : 1.0 / n;
-        dd[a] = w / m->S0_vec[a] * (gf * Sf[a] - gc * Sc[a]);
+        double w = (m->weights && !dup) ? m->weights[a] : 1.0 / n;
+        dd[a] = (dup && !own) ? 0.0 : w / m->S0_vec[a] * (gf * Sf[a] - gc * Sc[a]);
     }
     free(Sf);
     return yf;
@@ -813,7 +837,7 @@ int orc_basket_level_sums(const mcq_model* m, const mcq_payoff* p, int n_fine, i
             uint32_t idx = offset + (uint32_t)i;
             if (i > b) { int k = __builtin_ctz(idx); for (int q = 0; q < D; q++) x[q] ^= L[q * 33 + k]; }
             for (int q = 0; q < D; q++) z[q] = orc_ppnd16((double)orc_u_of(x[q], flags));
-            double yc, yf = orc_basket_level(m, p, n_fine, M, z, &yc, dd);
+            double yc, yf = orc_basket_level_f(m, p, n_fine, M, z, &yc, dd, flags);
             double dy = yf - yc;
             s[0] += dy; s[1] += dy * dy; s[2] += yf; s[3] += yf * yf;
             for (int a = 0; a < n; a++) s[4 + a] += dd[a];

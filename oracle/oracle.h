@@ -84,6 +84,8 @@ double orc_level_payoff(const mcq_model* m, const mcq_payoff* p, int n_fine, int
 /* coupled correlated GBM basket call with pathwise d(dY)/dS0_a in dd[n_assets]; M <= 0: level 0 */
 double orc_basket_level(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, const double* z,
                         double* yc, double* dd);
+double orc_basket_level_f(const mcq_model* m, const mcq_payoff* p, int n_fine, int M, const double* z,
+                          double* yc, double* dd, int flags);
 
 /* ---- drivers (sums over replicas/points; OpenMP) ---- */
 /* sums[R][2]: {sum Y, sum Y^2} over points offset..offset+N-1 of salts salt_base + r */

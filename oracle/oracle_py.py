@@ -58,6 +58,9 @@ def lib():
         L.orc_u_of.restype = C.c_float
         L.orc_u_of.argtypes = [C.c_uint32, C.c_int]
         L.orc_path_payoff.restype = C.c_double
+        L.orc_path_payoff_f.restype = C.c_double
+        L.orc_basket_level_f.restype = C.c_double
+        L.orc_is_payoff.restype = C.c_double
         L.orc_level_payoff.restype = C.c_double
         _lib = L
     return _lib
@@ -160,10 +163,10 @@ def sobol_hh_normal(salt, dim0, nd, offset, n, flags=0):
     return out
 
 
-def path_payoff(m, p, n_steps, z, nz=None):
+def path_payoff(m, p, n_steps, z, nz=None, flags=0):
     z = np.ascontiguousarray(z, dtype=np.float64)
-    return lib().orc_path_payoff(C.byref(m), C.byref(p), C.c_int(n_steps), C.byref(nz) if nz else None,
-                                 z.ctypes.data_as(_pd))
+    return lib().orc_path_payoff_f(C.byref(m), C.byref(p), C.c_int(n_steps), C.byref(nz) if nz else None,
+                                   z.ctypes.data_as(_pd), C.c_int(flags))
 
 
 def qmc_sums(m, p, n_steps, nz=None, salt_base=42, R=1, offset=0, N=1024, flags=0, threads=0):
@@ -186,15 +189,16 @@ def level_sums(m, p, n_fine, M, nz=None, use_sobol=True, seed=42, salt_base=42, 
     return out
 
 
-def basket_level(m, p, n_fine, M, z):
-    """One coupled basket path pair: (Yf, Yc, dd[n_assets]); M <= 0 is level 0."""
+def basket_level(m, p, n_fine, M, z, flags=0):
+    """One coupled basket path pair (GBM or Dupire basket): (Yf, Yc, dd[n_assets]); M <= 0 is
+    level 0."""
     z = np.ascontiguousarray(z, dtype=np.float64)
     dd = np.zeros(m.n_assets)
     yc = C.c_double()
     L = lib()
-    L.orc_basket_level.restype = C.c_double
-    yf = L.orc_basket_level(C.byref(m), C.byref(p), C.c_int(n_fine), C.c_int(M), z.ctypes.data_as(_pd),
-                            C.byref(yc), dd.ctypes.data_as(_pd))
+    L.orc_basket_level_f.restype = C.c_double
+    yf = L.orc_basket_level_f(C.byref(m), C.byref(p), C.c_int(n_fine), C.c_int(M), z.ctypes.data_as(_pd),
+                              C.byref(yc), dd.ctypes.data_as(_pd), C.c_int(flags))
     return yf, yc.value, dd
 
 

@@ -149,3 +149,55 @@ def test_book_object_copies_and_validates(eng):
     out = (eng.mcq_types.BookResult * 1)()
     assert L.mcq_book_run(b.h, C.byref(ml), C.byref(qc), 0, out, None) == 1   # empty book
     b.close()
+
+
+@pytest.mark.parametrize("M", [0, 2, 4])
+def test_oracle_dupire_basket_own_s0_deltas_vs_fd(eng, orc, M):
+    """Dupire basket with each asset's volatility scaled by its own S0 (MCQ_FLAG_BASKET_OWN_S0): the
+    path is homogeneous of degree one in (S0_a, S_a), so dd[a] = w_a / S0_a (gf Sf_a - gc Sc_a) is
+    the total derivative of the coupled pair dY with respect to S0_a (the scale moving too).  FP64
+    central differences path by path; with the reference's asset-0 scale the deltas are 0."""
+    d = 4
+    S0, _, Lc, _ = _basket_model(eng, d, 7)
+    K, r, T, n_fine = float(S0.mean()), 0.03, 1.0, 8
+    p = eng.basket(K, r, T, d)
+    F = eng.FLAG_BASKET_OWN_S0
+    rng = np.random.default_rng(5)
+    h = 1e-5
+    checked = 0
+    for _ in range(30):
+        z = rng.normal(size=n_fine * d)
+        m = eng.multi_dupire(S0, Lc, mu=r, T=T)
+        yf, yc, dd = orc.basket_level(m, p, n_fine, M, z, flags=F)
+        _, _, dd0 = orc.basket_level(m, p, n_fine, M, z)
+        assert not dd0.any()
+        for a in range(d):
+            up, dn = S0.copy(), S0.copy()
+            up[a] += h
+            dn[a] -= h
+            fu, cu, _ = orc.basket_level(eng.multi_dupire(up, Lc, mu=r, T=T), p, n_fine, M, z, flags=F)
+            fd, cd, _ = orc.basket_level(eng.multi_dupire(dn, Lc, mu=r, T=T), p, n_fine, M, z, flags=F)
+            if (fu == 0.0) != (fd == 0.0) or (M > 0 and (cu == 0.0) != (cd == 0.0)):
+                continue
+            fdiff = ((fu - cu) - (fd - cd)) / (2 * h)
+            assert abs(fdiff - dd[a]) < 1e-6 * (1 + abs(dd[a])), (a, fdiff, dd[a])
+            checked += 1
+    assert checked > 10 * d
+
+
+def test_oracle_dupire_basket_level0_matches_the_uncoupled_path(eng, orc):
+    """Level 0 of the coupled Dupire basket pair is the reference's plain Dupire basket path
+    (kernel_multi_dupire, asset 0's S0 in every asset's volatility), and the own-S0 flag reaches
+    both."""
+    S0, _, Lc, _ = _basket_model(eng, 3, 9)
+    m = eng.multi_dupire(S0, Lc, mu=0.03, T=1.5)
+    p = eng.basket(float(S0.mean()), 0.03, 1.5, 3)
+    z = np.random.default_rng(6).normal(size=16 * 3)
+    vals = []
+    for flags in (0, eng.FLAG_BASKET_OWN_S0):
+        yf, yc, _ = orc.basket_level(m, p, 16, 0, z, flags=flags)
+        assert yc == 0.0
+        ref = orc.path_payoff(m, p, 16, z, flags=flags)
+        assert abs(yf - ref) < 1e-12 * (1 + abs(yf)), (flags, yf, ref)
+        vals.append(yf)
+    assert vals[0] != vals[1]

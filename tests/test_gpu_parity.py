@@ -275,3 +275,69 @@ def test_is_pass_vs_oracle(gpu, orc, use_sobol, K, z_star, n_steps):
     # the shift and the likelihood ratio are applied: the sums differ from those of z* = 0
     g0 = gpu.is_pass(m, p, n_steps, 0.0, use_sobol=use_sobol, seed=9, salt_base=31, R=R, offset=17, n_points=N)
     assert np.abs(g0[:, 0] - g[:, 0]).max() > 1e-3 * np.abs(g[:, 0]).max()
+
+
+def _corr_basket(n, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((n, n))
+    Cm = A @ A.T + 0.5 * np.eye(n)
+    d = np.sqrt(np.diag(Cm))
+    return 100 * rng.uniform(0.8, 1.2, n), np.linalg.cholesky(Cm / np.outer(d, d))
+
+
+@pytest.mark.parametrize("flags", [0, 16])
+@pytest.mark.parametrize("n", [1, 3, 8, 16])
+@pytest.mark.parametrize("level,M", [(0, 2), (1, 2), (3, 2), (1, 4), (2, 4)])
+def test_dupire_basket_level_pass(gpu, orc, n, level, M, flags):
+    """The coupled Dupire basket (the reference's kernel_multi_dupire path stepped as kernel_mlmc
+    steps a one-asset Dupire path; the reference refuses it at methods_cuda.cu:1318-1320) against the
+    FP64 oracle's pair on the same scrambled points, with the reference's asset-0 volatility scale
+    and with MCQ_FLAG_BASKET_OWN_S0 (16)."""
+    S0, L = _corr_basket(n, 40 + n)
+    m = gpu.multi_dupire(S0, L, mu=0.04, T=1.0)
+    p = gpu.basket(float(S0.mean()), 0.04, 1.0, n)
+    nf = M ** level
+    R, N = 2, 512
+    g = gpu.level_pass(m, p, nf, M if level else 0, use_sobol=True, salt_base=70, R=R, offset=9, n_points=N,
+                       flags=flags)
+    o = orc.basket_level_sums(m, p, nf, M if level else 0, salt_base=70, R=R, offset=9, N=N, flags=flags)
+    for r in range(R):
+        sc = 1 + abs(o[r, 2] / N)
+        assert abs(g[r, 0] / N - o[r, 0] / N) < 3e-4 * sc, (r, g[r], o[r, :4])
+        assert abs(g[r, 2] / N - o[r, 2] / N) < 3e-4 * sc, (r, g[r], o[r, :4])
+
+
+def test_dupire_basket_own_s0_single_level(gpu, orc):
+    """MCQ_FLAG_BASKET_OWN_S0 in the single-level Dupire basket pass (BasketC and the wide basket):
+    against the oracle with the flag, and different from the reference's asset-0 scale."""
+    for n in (5, 40):
+        S0, L = _corr_basket(n, 3)
+        m = gpu.multi_dupire(S0, L, mu=0.04, T=1.0)
+        p = gpu.basket(float(S0.mean()), 0.04, 1.0, n)
+        R, N, steps = 2, 256, 8
+        got = {}
+        for flags in (0, gpu.FLAG_BASKET_OWN_S0):
+            g = gpu.qmc_pass(m, p, steps, salt_base=21, R=R, offset=0, n_points=N, flags=flags)
+            o = orc.qmc_sums(m, p, steps, None, salt_base=21, R=R, offset=0, N=N, flags=flags)
+            for r in range(R):
+                assert abs(g[r, 0] / N - o[r, 0] / N) < 3e-4 * (1 + abs(o[r, 0] / N)), (n, flags, g[r], o[r])
+            got[flags] = g
+        assert np.abs(got[0][:, 0] - got[gpu.FLAG_BASKET_OWN_S0][:, 0]).max() > 1e-6 * N
+
+
+@pytest.mark.parametrize("flags", [0, 16])
+def test_dupire_basket_mlmc_mlqmc(gpu, flags):
+    """MLMC and MLQMC of a 4-asset Dupire basket (refused by the reference) telescope to the plain
+    estimator at their finest level: compared with it within 3 standard
+    errors of the difference plus the bias bound eps / sqrt(2) of the stopping test (the plain
+    estimator: single-level RQMC at that step count, independent salts)."""
+    S0, L = _corr_basket(4, 8)
+    m = gpu.multi_dupire(S0, L, mu=0.03, T=1.0)
+    p = gpu.basket(float(S0.mean()), 0.03, 1.0, 4)
+    eps = 2e-2
+    ml = gpu.run_mlmc(m, p, eps, gpu.mlmc_cfg(M=2, max_L=8, flags=flags))
+    q = gpu.run_mlqmc(m, p, eps, gpu.mlmc_cfg(M=2, max_L=8, flags=flags), gpu.qmc_cfg(R=16, flags=flags))
+    for r in (ml, q):
+        finest = 2 ** (r["levels"] - 1)
+        ref = gpu.run_qmc(m, p, eps / 2, finest, gpu.qmc_cfg(R=16, N0_per_replica=1 << 12, salt_base=900, flags=flags))
+        assert abs(r["price"] - ref["price"]) < 3 * np.hypot(r["std_error"], ref["std_error"]) + eps / np.sqrt(2), (r, ref)
