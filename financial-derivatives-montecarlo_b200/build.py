@@ -57,7 +57,7 @@ def build(force=False, jobs=None, verbose_ptxas=False, quiet=False):
     objs = [os.path.join(BUILD, s + ".o") for s in srcs]
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
-            "-L", os.path.join(CUDA, "lib64"), "-lcurand", "-Xlinker", "-rpath," + os.path.join(CUDA, "lib64")]
+            "-L", os.path.join(CUDA, "lib64"), "-lcurand", "-lcublas", "-Xlinker", "-rpath," + os.path.join(CUDA, "lib64")]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

@@ -17,6 +17,7 @@ const void* lookup_sobol_bb(int model, int payoff, bool coupled);
 const void* lookup_sobol_bb_b3(int model, int payoff);          // 3-CTA (80-register) variant
 const void* lookup_sobol_bbu(int model, int payoff, bool coupled, int variant);   // NOISE_BB_UNI
 const void* lookup_sobol_pca_small(int model, int payoff, bool coupled);   // N <= 32
+const void* lookup_dw(int model, int payoff, bool coupled);   // NOISE_DW (large-N PCA increments)
 const void* lookup_philox_plain(int model, int payoff);
 const void* lookup_philox_coupled(int model, int payoff);
 // est in {EST_CV_ASIAN, EST_CV_DUPIRE, EST_IS}, basket models (nb = 4, 8, 16), dump probes

@@ -259,8 +259,9 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
     if (m.kind == MCQ_MODEL_MULTI_DUPIRE || m.kind == MCQ_MODEL_BASKET_GBM) {
         const int n = m.n_assets;
         MCQ_REQUIRE(n >= 1, MCQ_ERR_INVALID, "basket needs n_assets >= 1");
-        MCQ_REQUIRE(n <= 128, MCQ_ERR_UNSUPPORTED,
-                    "basket width " + std::to_string(n) + " exceeds the limit of 128 assets");
+        MCQ_REQUIRE(n <= kMaxHugeBasket, MCQ_ERR_UNSUPPORTED,
+                    "basket width " + std::to_string(n) + " exceeds the limit of " + std::to_string(kMaxHugeBasket) +
+                        " assets");
         MCQ_REQUIRE(m.S0_vec != nullptr, MCQ_ERR_INVALID, "basket needs S0_vec");
         if (m.kind == MCQ_MODEL_BASKET_GBM)
             MCQ_REQUIRE(m.sigma_vec != nullptr, MCQ_ERR_INVALID, "basket needs sigma_vec");
@@ -357,16 +358,22 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     }
     // the kernel family: the bridge with uniform window weights reads them from the parameters
     const int knoise = (a.noise == NOISE_BB && D > 32 && a.bb->bb_uni) ? NOISE_BB_UNI : a.noise;
-    const bool pca_tc = (a.noise == NOISE_PCA) && D >= 64;
+    const bool pca_tc = (a.noise == NOISE_PCA) && (D == 64 || D == 128 || D == 256);
     if (a.noise == NOISE_PCA) {
         MCQ_REQUIRE(k.d_noise == 1, MCQ_ERR_UNSUPPORTED, "PCA needs a one-factor model");
         MCQ_REQUIRE(a.gen == GEN_SOBOL, MCQ_ERR_UNSUPPORTED, "PCA is a QMC transform");
         MCQ_REQUIRE(a.pca && a.pca->kind == MCQ_NOISE_PCA && a.pca->n == a.n_steps, MCQ_ERR_INVALID,
                     "PCA handle missing or built for a different step count");
-        MCQ_REQUIRE(D <= 32 || D == 64 || D == 128 || D == 256, MCQ_ERR_UNSUPPORTED,
-                    "fused PCA supports N <= 32 and N in {64, 128, 256} steps; got " + std::to_string(D));
         k.pca = a.pca->table.p;
     }
+    // fused: N <= 32 inside k_pass, N in {64, 128, 256} in the tensor-core pass (its factor in
+    // shared memory); other N through fp16 normals, a library GEMM and the pass on increments
+    if (a.noise == NOISE_PCA && D > 32 && D != 64 && D != 128 && D != 256 && !a.dump) {
+        pca_large_pass_async(ws, a, k, d_out);
+        return;
+    }
+    MCQ_REQUIRE(!(a.noise == NOISE_PCA && a.dump) || D <= 32 || D == 64 || D == 128 || D == 256,
+                MCQ_ERR_UNSUPPORTED, "the PCA dump probe covers N <= 32 and N in {64, 128, 256}");
     if (pca_tc) {
         pca_pass_async(ws, a, k, d_out);
         return;

@@ -61,6 +61,11 @@ struct Workspace {
     PinnedBuf hsums, haux;
     DevBuf xbuf[8];       // long-lived scratch of the batched book (book.cu): kept across calls
     PinnedBuf xpin[2];
+    DevBuf pca_z, pca_dw, pca_tmp;   // the large-N PCA route (pca_large.cu): fp16 normals, increments
+    struct Blas {                    // its cuBLAS handle, created on first use
+        void* h = nullptr;
+        ~Blas();
+    } blas;
     uint32_t dirs_salt0 = 0;
     int dirs_R = -1, dirs_D = -1;
     void ensure_stream();
@@ -158,6 +163,9 @@ int nstat_of(int est, int model_kind);   // basket levels carry per-asset deltas
 void pass_async(Workspace& ws, const PassArgs& a, double* d_out);
 // Tensor-core PCA pass (N in {64, 128, 256}); called by pass_async.
 void pca_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out);
+// PCA orderings the tensor-core pass does not hold (N > 32 outside {64, 128, 256}): fp16 normals,
+// one library GEMM and the fused pass on the increments, batch by batch (pca_large.cu)
+void pca_large_pass_async(Workspace& ws, const PassArgs& a, KParams& k, double* d_out);
 // Enqueue, copy back and wait; returns [R][nstat].
 std::vector<double> pass_sync(Workspace& ws, const PassArgs& a);
 // After a synchronisation of ws.stream: raises MCQ_ERR_TIMEOUT if a bounded device-side wait of

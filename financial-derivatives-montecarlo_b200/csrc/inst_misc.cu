@@ -30,6 +30,7 @@ static const void* misc_gen(int noise, int est, int model, int nb, bool dump) {
         if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_MULTI, 8>>;
         if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_MULTI, 16>>;
         if (nb <= kMaxWideBasket) return (const void*)&k_pass<GEN, NOISE_RAW, BasketWideC<MOD_MULTI>>;
+        if (nb <= kMaxHugeBasket) return (const void*)&k_pass<GEN, NOISE_RAW, BasketWideC<MOD_MULTI, kMaxHugeBasket>>;
         return nullptr;
     }
     if (model == MOD_BASKET) {
@@ -37,6 +38,7 @@ static const void* misc_gen(int noise, int est, int model, int nb, bool dump) {
         if (nb <= 8) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_BASKET, 8>>;
         if (nb <= 16) return (const void*)&k_pass<GEN, NOISE_RAW, BasketC<MOD_BASKET, 16>>;
         if (nb <= kMaxWideBasket) return (const void*)&k_pass<GEN, NOISE_RAW, BasketWideC<MOD_BASKET>>;
+        if (nb <= kMaxHugeBasket) return (const void*)&k_pass<GEN, NOISE_RAW, BasketWideC<MOD_BASKET, kMaxHugeBasket>>;
         return nullptr;
     }
     return nullptr;

@@ -19,7 +19,10 @@ enum Gen : int { GEN_SOBOL = 0, GEN_PHILOX = 1 };
 // normal tiles by three helper warps (engine-internal as well)
 // NOISE_BB_UNI: the Brownian bridge whose window weights are the same for every point of a level
 // (read from KParams::bbw instead of the per-dimension table; engine-internal)
-enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3, NOISE_ASSIST = 4, NOISE_BB_UNI = 5 };
+// NOISE_DW: time-ordered increments computed outside the pass (the PCA orderings whose factor does
+// not fit the tensor-core kernel's shared memory), read from KParams::dw_in (engine-internal)
+enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3, NOISE_ASSIST = 4, NOISE_BB_UNI = 5,
+                   NOISE_DW = 6 };
 
 // Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
 constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
@@ -32,6 +35,8 @@ enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE
 constexpr int kWarpsPerBlock = 8;
 constexpr int kThreads = kWarpsPerBlock * 32;
 constexpr int kMaxBasket = 16;          // register-resident basket width
+constexpr int kMaxWideBasket = 128;     // wide baskets: per-asset state in local memory
+constexpr int kMaxHugeBasket = 1024;    // widest (the reference's 1000-asset example)
 constexpr int kMinBlocks = 3;           // resident CTAs per SM the register budget is set for
 constexpr int kMaxStats = 8;
 // Assisted passes (NOISE_ASSIST): per owner warp, three helper warps and a ring of four 32 x 32
@@ -103,6 +108,9 @@ struct KParams {
     double* node_out;
     // ---- bounded-wait / error reporting
     int* err;
+    // ---- NOISE_DW: increment i of point offset + row at dw_in[i * dw_stride + row]
+    const float* dw_in;
+    int dw_stride;
 };
 
 }  // namespace mcq

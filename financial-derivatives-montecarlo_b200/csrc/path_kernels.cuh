@@ -732,13 +732,13 @@ struct BasketLevelC {
     }
 };
 
-// Wide basket (up to kMaxWideBasket assets, e.g. the reference's 100-asset example): the same
-// arithmetic as BasketC with the per-asset state in local memory and rolled loops.
-constexpr int kMaxWideBasket = 128;
-template <int MOD>
+// Wide basket (up to NMAX assets: kMaxWideBasket for the reference's 100-asset example,
+// kMaxHugeBasket for its 1000-asset uncorrelated one): the same arithmetic as BasketC with the
+// per-asset state in local memory and rolled loops.
+template <int MOD, int NMAX = kMaxWideBasket>
 struct BasketWideC {
     static constexpr int NST = 2;
-    float S[kMaxWideBasket], dw[kMaxWideBasket];
+    float S[NMAX], dw[NMAX];
     float muh;
     int f, k;
     __device__ __forceinline__ void bind(int, uint64_t) {}
@@ -883,6 +883,19 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
             cons.step_dw(p, acc, 0.f);
         }
         cons.flush();
+    } else if constexpr (NOISE == NOISE_DW) {
+        // increments produced outside the pass (the large-N PCA product), time-ordered in
+        // p.dw_in[i * p.dw_stride + row] for the point offset + row; lanes of a group read
+        // consecutive rows (coalesced).  Lanes outside the point range step on zeros.
+        const bool valid = n >= p.offset && n < p.offset + p.n_points;
+        const float* col = p.dw_in + (valid ? (size_t)(n - p.offset) : (size_t)0);
+        for (int t0 = 0; t0 < D; t0 += 32) {
+            const int nv = min(32, D - t0);
+#pragma unroll 4
+            for (int i = 0; i < nv; i++)
+                cons.step_dw(p, valid ? __ldg(col + (size_t)(t0 + i) * (size_t)p.dw_stride) : 0.f, 0.f);
+            cons.flush();
+        }
     } else {   // NOISE_BB, one factor: D == n_steps == N (power of two)
         // Bridge table row j (Sobol dimension j = bb_precompute step j, utils.cpp:54-101):
         // p.bb[j] = {wl, wr, sd, bits(m)} and p.bbi[j] = {l, r}: W[m] = wl W[l] + wr W[r] + sd z_j.

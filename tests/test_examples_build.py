@@ -1,7 +1,8 @@
 """The reference's own example programs compile and link unchanged against include/mcq.hpp and
 libmcq.so (the drop-in claim for C++ callers).  Each example is built from a scratch copy whose
 `../methods_cuda.cuh` is a one-line shim including mcq.hpp; nothing of the reference is kept.
-Skipped where the reference sources are absent."""
+Skipped where the reference sources are absent (their location: $MCQ_REFERENCE_DIR, default
+/root/reference)."""
 import glob
 import os
 import shutil
@@ -11,7 +12,7 @@ import tempfile
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_EX = "/root/reference/examples"
+REF_EX = os.path.join(os.environ.get("MCQ_REFERENCE_DIR", "/root/reference"), "examples")
 LIBDIR = os.path.join(ROOT, "financial-derivatives-montecarlo_b200")
 
 

@@ -127,3 +127,39 @@ def test_pca_ragged_ranges_add_up(gpu):
                 for a, b in [(5, 133), (133, 134), (134, 50001), (50001, 100006)])
     np.testing.assert_allclose(parts, whole, rtol=2e-6)
     pca.close()
+
+
+@pytest.mark.parametrize("N", [48, 100, 512, 1024])
+@pytest.mark.parametrize("pay", ["asian", "eur"])
+def test_pca_large_n_pass_vs_oracle(gpu, orc, N, pay):
+    """PCA orderings outside the tensor-core pass's sizes (fp16 normals, the library GEMM of the
+    reference's phase1_pca, the fused pass on the increments) against the FP64 oracle's product of
+    the same fp16-rounded factor and normals."""
+    m = gpu.gbm(100.0, 0.03, 0.25, 1.0)
+    p = gpu.asian(100.0) if pay == "asian" else gpu.european(100.0, 0.03, 1.0)
+    pca = gpu.pca_create(N, 1.0)
+    R, Np = 2, 1024 if N <= 512 else 256
+    g = gpu.qmc_pass(m, p, N, noise=gpu.PCA, pca=pca, salt_base=42, R=R, offset=5, n_points=Np)
+    o = orc.qmc_sums(m, p, N, orc.noise(orc.T.PCA, N, 1.0), salt_base=42, R=R, offset=5, N=Np)
+    for r in range(R):
+        assert abs(g[r, 0] / Np - o[r, 0] / Np) < 3e-4 * (1 + abs(o[r, 0] / Np)), (r, g[r], o[r])
+    pca.close()
+
+
+def test_pca_large_n_batches_and_levels(gpu):
+    """A 2048-step PCA pass larger than one batch (2^27 / N points) equals the sum of its two halves
+    priced separately (only the FP64 summation order differs), and a coupled MLQMC level at 512
+    steps runs through the same route."""
+    m, p = gpu.gbm(100.0, 0.03, 0.25, 1.0), gpu.asian(100.0)
+    N = 2048
+    pca = gpu.pca_create(N, 1.0)
+    n1 = (1 << 27) // N
+    whole = gpu.qmc_pass(m, p, N, noise=gpu.PCA, pca=pca, salt_base=3, R=1, offset=0, n_points=n1 + 1000)
+    a = gpu.qmc_pass(m, p, N, noise=gpu.PCA, pca=pca, salt_base=3, R=1, offset=0, n_points=n1)
+    b = gpu.qmc_pass(m, p, N, noise=gpu.PCA, pca=pca, salt_base=3, R=1, offset=n1, n_points=1000)
+    assert np.allclose(whole, a + b, rtol=1e-12, atol=0), (whole, a + b)
+    pca.close()
+    pl = gpu.pca_create(512, 1.0)
+    lv = gpu.level_pass(m, p, 512, 2, noise=gpu.PCA, pca=pl, salt_base=5, R=2, n_points=2048)
+    assert np.all(np.isfinite(lv)) and np.all(np.abs(lv[:, 0] / 2048) < 0.05)   # the level difference is small
+    pl.close()
