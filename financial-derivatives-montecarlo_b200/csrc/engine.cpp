@@ -210,7 +210,10 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
     k.v0 = (float)m.v0;
     k.L10 = (float)m.hes_L10;
     k.L11 = (float)m.hes_L11;
-    k.em_f = (float)std::exp((double)(-k.kappa * h));
+    // 1 - e^{-kappa h} with its own relative precision: at fine levels e^{-kappa h} lies within a few
+    // FP32 ulps of 1, and rounding it there biases the mean reversion by up to 0.4 % at 2^18 steps
+    // (the reference rounds expf(-kappa h) itself, methods_cuda.cu:282)
+    k.om_f = (float)(-std::expm1(-(double)k.kappa * (double)h));
     k.sigma0 = (float)m.sigma0;
     k.alpha = (float)m.alpha;
     k.bm1 = (float)m.beta_d - 1.0f;
@@ -220,13 +223,11 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
         k.M = a.M;
         k.n_coarse = a.level0 ? 0 : a.n_steps / a.M;
         k.hc = (float)(m.T / std::max(k.n_coarse, 1));
-        k.em_c = (float)std::exp((double)(-k.kappa * k.hc));
+        k.om_c = (float)(-std::expm1(-(double)k.kappa * (double)k.hc));
         if (a.level0) k.M = INT_MAX;   // the coarse path never steps on level 0
     }
     if (m.kind == MCQ_MODEL_HESTON && (a.flags & MCQ_FLAG_HESTON_MILSTEIN)) {
         k.mil = 0.25f * k.xi * k.xi;
-        k.mil_hf = k.mil * k.h;
-        k.mil_hc = k.mil * (k.hc > 0.f ? k.hc : k.h);
     }
 
     k.K = (float)p.K;

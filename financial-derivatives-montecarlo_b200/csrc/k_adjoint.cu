@@ -264,11 +264,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
 __device__ __forceinline__ void heston_adj_step(const KParams& p, float& S, float& V, float dw1, float dw2,
                                                 float muh) {
     const float sq = sqrtf(fmaxf(V, 0.f));
-    S = fmaf(sq * S, dw1, fmaf(muh, S, S));   // the pricing pass's operations (Leg::step)
-    V = fmaf(p.xi * sq, dw2, fmaf(p.em_f, V - p.theta, p.theta));
-    // Milstein term only with the flag (mil != 0): fmaf(0, dW^2, V) would turn an infinite
-    // normal (reference-compat u = 1 point) into NaN
-    V = (p.mil != 0.f) ? fmaf(p.mil, dw2 * dw2, V - p.mil_hf) : V;
+    // the pricing pass's operations (Leg::step): one rounding against S and one against V
+    S = fmaf(S, fmaf(sq, dw1, muh), S);
+    float inc = fmaf(p.xi * sq, dw2, p.om_f * (p.theta - V));
+    inc = (p.mil != 0.f) ? fmaf(p.mil, fmaf(dw2, dw2, -p.h), inc) : inc;
+    V = V + inc;
 }
 
 template <int PAY>
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_adjoint_heston(const __grid_con
                     const float sq = sqrtf(fmaxf(Vk, 0.f));
                     const float dsq = (Vk > 0.f) ? 0.5f / sq : 0.f;
                     mubar = fmaf(Sbar, Sk * h, mubar);
-                    const float nV = fmaf(Sbar, Sk * dw1 * dsq, Vbar * fmaf(p.xi * dw2, dsq, p.em_f));
+                    const float nV = fmaf(Sbar, Sk * dw1 * dsq, Vbar * fmaf(p.xi * dw2, dsq, 1.f - p.om_f));
                     float direct = 0.f;
                     if constexpr (PAY == PAY_ASIAN) direct = (k >= 1) ? g_all : 0.f;
                     if constexpr (PAY == PAY_LOOKBACK) direct = (k == kmin) ? -p.corr_f : 0.f;

@@ -26,8 +26,9 @@ enum Noise : int { NOISE_RAW = 0, NOISE_BB = 1, NOISE_PCA = 2, NOISE_PACKED = 3,
 
 // Status written to KParams::err when a bounded device wait gives up (MCQ_ERR_TIMEOUT).
 constexpr int MCQ_ERR_TIMEOUT_CODE = 7;
-// MCQ_FLAG_BASKET_OWN_S0 as the kernels test it in KParams::flags.
+// MCQ_FLAG_BASKET_OWN_S0 and MCQ_FLAG_COMPAT_U_INF as the kernels test them in KParams::flags.
 constexpr int MCQ_FLAG_OWN_S0_CODE = 16;
+constexpr int MCQ_FLAG_COMPAT_U_INF_CODE = 1;
 enum ModelK : int { MOD_GBM = 0, MOD_HESTON = 1, MOD_DUPIRE = 2, MOD_MULTI = 3, MOD_LVGRID = 4, MOD_BASKET = 5 };
 enum PayK : int { PAY_EUR = 0, PAY_ASIAN = 1, PAY_GEOM = 2, PAY_LOOKBACK = 3, PAY_UPOUT = 4, PAY_BASKET = 5, PAY_DOWNOUT = 6 };
 enum Est : int { EST_PLAIN = 0, EST_COUPLED = 1, EST_CV_ASIAN = 2, EST_CV_DUPIRE = 3, EST_IS = 4 };
@@ -68,10 +69,10 @@ struct KParams {
     uint64_t G;         // groups per replica
     // ---- model (single precision, as the reference's c_p)
     float S0, inv_S0, mu, T, h, sqrt_h, sigma;
-    float kappa, theta, xi, L10, L11, v0, em_f;    // em_f = exp(-kappa h)
+    float kappa, theta, xi, L10, L11, v0, om_f;    // om_f = 1 - exp(-kappa h), from expm1
     float sigma0, alpha, bm1;                      // Dupire: bm1 = beta_d - 1
-    float hc, em_c;                                // coarse step, exp(-kappa hc)
-    float mil, mil_hf, mil_hc;                     // Heston Milstein: xi^2/4 and its h, hc multiples (0: Euler)
+    float hc, om_c;                                // coarse step, 1 - exp(-kappa hc)
+    float mil;                                     // Heston Milstein: xi^2/4 (0: Euler)
     // ---- payoff
     float K, B, disc, corr_f, corr_c, u_cap;
     float pay_T;                                   // payoff maturity (discount sensitivity)

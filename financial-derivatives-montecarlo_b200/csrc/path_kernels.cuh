@@ -278,7 +278,7 @@ struct Leg {
     }
     template <bool RUN>
     __device__ __forceinline__ void step(const KParams& p, float dw1, float dw2, float t,
-                                         float muh, float em, float milh) {
+                                         float muh, float omk, float hstep) {
         if constexpr (MOD == MOD_GBM) {
             S = fmaf(S, fmaf(p.sigma, dw1, muh), S);
         } else if constexpr (MOD == MOD_DUPIRE) {
@@ -288,17 +288,30 @@ struct Leg {
             const float sl = lv_sigma(p, S, t);
             S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_HESTON) {
-            // S + mu h S + (sqrt(V+) S) dW1 with the reference's product sqrt(V+) S (:280): a path
-            // that went infinite (reference-compat u = 1 point) and whose variance truncates to 0
-            // then becomes NaN (0 * inf) as the reference's does, not +inf
+            // S + S (mu h + sqrt(V+) dW1): the drift joins the random increment before the one
+            // rounding against S (S + mu h S rounded on its own would quantise the drift of a fine
+            // step, a few ulps of S, the same way at every step: a bias at 2^18 steps)
             const float sq = sqrtf(fmaxf(V, 0.f));
-            S = fmaf(sq * S, dw1, fmaf(muh, S, S));
-            V = fmaf(p.xi * sq, dw2, fmaf(em, V - p.theta, p.theta));
-            // Milstein: xi^2/4 (dW^2 - h), selected by the parameter block (a uniform predicate,
-            // no branch per step).  Without the flag V is kept as it is: an unconditional
-            // fmaf(0, dW^2, V) would turn the +inf normal of the reference-compat u = 1 point
-            // into NaN, where the reference's Euler step keeps V = +inf.
-            V = (p.mil != 0.f) ? fmaf(p.mil, dw2 * dw2, V - milh) : V;
+            const float Sp = S;
+            S = fmaf(S, fmaf(sq, dw1, muh), S);
+            if (p.flags & MCQ_FLAG_COMPAT_U_INF_CODE) {
+                // reference-compat: a path that went infinite (u = 1 point) and whose variance
+                // truncates to 0 becomes NaN through the reference's product sqrt(V+) S (:280)
+                const float t0 = sq * Sp;
+                if (t0 != t0) S = t0;
+            }
+            // V + (1 - e^{-kappa h}) (theta - V) + xi sqrt(V+) dW2 (+ xi^2/4 (dW2^2 - h) with the
+            // Milstein flag): the reference's exact-mean Euler step (:282-283) with 1 - e^{-kappa h}
+            // at full relative precision, and every term summed into one increment before the one
+            // rounding against V.  A deterministic term rounded against V on its own (V - xi^2 h / 4,
+            // or V + (1 - e^{-kappa h})(theta - V)) leaves the same fraction of an ulp every fine
+            // step: at 2^18 steps a drift of V of ~0.5 % that the level differences do not cancel.
+            // The Milstein choice is a select on the parameter block (no branch per step); without
+            // the flag the term is not formed at all, so an infinite normal of the reference-compat
+            // u = 1 point leaves V = +inf as the reference's step does, not 0 * inf = NaN.
+            float inc = fmaf(p.xi * sq, dw2, omk * (p.theta - V));
+            inc = (p.mil != 0.f) ? fmaf(p.mil, fmaf(dw2, dw2, -hstep), inc) : inc;
+            V = V + inc;
         }
         if constexpr (RUN && path_dep<PAY>()) update();
     }
@@ -341,10 +354,10 @@ struct PathC {
     __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
         const float t = (float)k * p.h;
         if constexpr (HES && COUPLED) {   // run_upd is a runtime flag only here
-            f.template step<false>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
+            f.template step<false>(p, dw1, dw2, t, muh_f, p.om_f, p.h);
             if constexpr (path_dep<PAY>()) f.update_if(run_upd);
         } else {
-            f.template step<true>(p, dw1, dw2, t, muh_f, p.em_f, p.mil_hf);
+            f.template step<true>(p, dw1, dw2, t, muh_f, p.om_f, p.h);
         }
         k++;
         if constexpr (COUPLED) {
@@ -353,10 +366,10 @@ struct PathC {
             if (++m == p.M) {
                 const float tc = (float)ck * p.hc;
                 if constexpr (HES) {
-                    c.template step<false>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
+                    c.template step<false>(p, a1, a2, tc, muh_c, p.om_c, p.hc);
                     if constexpr (path_dep<PAY>()) c.update_if(run_upd);
                 } else {
-                    c.template step<true>(p, a1, a2, tc, muh_c, p.em_c, p.mil_hc);
+                    c.template step<true>(p, a1, a2, tc, muh_c, p.om_c, p.hc);
                 }
                 a1 = a2 = 0.f; m = 0; ck++;
             }

@@ -6,8 +6,7 @@ it, runs its MC / MLMC / QMC / MLQMC / CV / IS drivers and prints the reference'
 table is read back with the reference report script's regexes (gen_informe.py:16-21).  The
 reference's own check of a row is |price - reference| < 2 eps (SI); a driver's result carries its
 statistical error besides the bias its step count was sized for, so every row must be within
-2 eps + 2 SE of the reference, and must say SI unless only that statistical allowance separates
-it (e.g. ejemplo02's pseudo-random MC row at the default eps: bias ~0.07 plus one SE of 0.035
+2 eps + 2 SE of the reference: SI, or NO by less than two standard errors (e.g. ejemplo02's pseudo-random MC row at the default eps: bias ~0.07 plus one SE of 0.035
 against 2 eps = 0.1).  Programs that are not built are skipped."""
 import os
 import re
@@ -45,5 +44,4 @@ def test_reference_example_runs_on_engine(name):
     for x in rows:
         assert int(x.group(4)) > 0 and float(x.group(3)) >= 0.0
         err, se = float(x.group(6)), float(x.group(3))
-        assert err < 2 * eps + 2 * se, (x.group(0), out)
-        assert x.group(7) == "SI" or err >= 2 * eps - 2 * se, (x.group(0), out)
+        assert err < 2 * eps + 2 * se, (x.group(0), out)   # SI, or NO by less than 2 SE
