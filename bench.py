@@ -21,6 +21,7 @@ cores on a bounded sample of the same workload (the reference has no CPU path of
 import argparse
 import importlib.util
 import json
+import math
 import os
 import subprocess
 import sys
@@ -32,11 +33,16 @@ PKG = os.path.join(ROOT, "financial-derivatives-montecarlo_b200")
 
 S0, K, R_, SIG, T_, STEPS, REPS, SALT = 100.0, 100.0, 0.03, 0.25, 1.0, 256, 32, 42
 METRIC = "path-steps/s"
-# Algorithmic FP32 work per path-step of the raw Sobol GBM Asian path (counted as written,
-# FMA = 2 flops): u from the scrambled integer (I2F, add, mul: 2 flops), the inverse normal as
-# one AS241 central-region rational (7 + 7 FMA + 1 div: 29 flops), the GBM step
-# S (1 + mu h + sigma sqrt(h) z) (2 FMA: 4 flops), the Kahan-compensated running sum (4 flops).
-FLOPS_PER_PATH_STEP = 2 + 29 + 4 + 4
+# Algorithmic FP32 work per path-step of the raw Sobol GBM Asian path, counted as written in the
+# reference (each +, -, x, /, min, max one flop; special functions apart): the scrambled-Sobol
+# normal's u = (x + 1) 2^-32 (2 flops) and one inverse normal (an SFU-class call, not counted as
+# flops), the GBM step S + mu S h + sigma S sqrt(h) z with the sqrt(h) scale (7 flops,
+# methods_cuda.cu:273), the Kahan-compensated running sum of the Asian average (4 flops).
+FLOPS_PER_PATH_STEP = 2 + 7 + 4
+SFU_PER_PATH_STEP = 1
+# The same path-step with the inverse normal counted as the AS241 central rational it evaluates
+# (7 + 7 FMA + 1 division: 29 flops): an issue model, not the algorithmic count.
+ISSUE_MODEL_FLOPS_PER_PATH_STEP = 2 + 29 + 4 + 4
 
 
 def load_engine():
@@ -115,6 +121,36 @@ def measured_peaks():
         return {}
 
 
+def oracle_values():
+    """FP64 oracle values of the benchmark's workloads (tests/golden/oracle_values.json, written by
+    tests/golden/make_oracle_values.py: closed forms where they exist, FP64 oracle runs otherwise)."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "oracle_values.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def vs_oracle(price, se, ref, ref_se=0.0, kind=""):
+    """A result's error against an FP64 oracle value, in absolute terms and in standard errors of
+    the difference."""
+    if ref is None:
+        return None
+    comb = math.hypot(se or 0.0, ref_se or 0.0)
+    return {"oracle": ref, "oracle_se": ref_se, "error": price - ref, "combined_se": comb,
+            "error_in_se": (price - ref) / comb if comb > 0 else None, "oracle_kind": kind}
+
+
+def bs_call(S0, K, T, r, sigma):
+    """Black–Scholes call in FP64 (the closed form the one-asset book options are checked against)."""
+    if T <= 0 or sigma <= 0:
+        return max(S0 - K * math.exp(-r * T), 0.0)
+    d1 = (math.log(S0 / K) + (r + 0.5 * sigma * sigma) * T) / (sigma * math.sqrt(T))
+    d2 = d1 - sigma * math.sqrt(T)
+    N = lambda x: 0.5 * math.erfc(-x / math.sqrt(2.0))   # noqa: E731
+    return S0 * N(d1) - K * math.exp(-r * T) * N(d2)
+
+
 def cpu_baseline(seconds=12.0, steps=1):
     """Oracle (CPU restatement, FP64 paths) on all host threads: returns path-steps/s."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -139,14 +175,15 @@ def cpu_baseline(seconds=12.0, steps=1):
             "sample": f"{REPS} replicas x {n} points x {STEPS} steps of the same workload (FP64 oracle)"}
 
 
-def configs_bench(eng):
+def configs_bench(eng, orv):
     """The other workloads of the benchmark suite through the public API, host wall time of one
-    warm call each: plain MC (GBM European, 64 Euler steps, Philox, pilot 2^14, eps 1e-2),
-    MLQMC for Heston with the Euler-Milstein full-truncation variance step (kappa 2, theta 0.04,
-    xi 0.3, rho -0.7, v0 0.04, S0 100, r 0.02, T 1; M 4, 4 steps on level 0, L <= 8, R 16,
-    eps 1e-3) with a lookback and a down-and-out call
-    (K 100, B 80), and the pathwise adjoint on the 64 x 32 local-vol grid (Asian call, T 2,
-    512 steps, 16 x 2^18 scrambled paths, price + delta + rho + 2048 node vegas)."""
+    warm call each, each result stated against its FP64 oracle value: plain MC (GBM European, 64
+    Euler steps, Philox, pilot 2^14, eps 1e-2; Black–Scholes), MLQMC for Heston with the
+    Euler-Milstein full-truncation variance step (kappa 2, theta 0.04, xi 0.3, rho -0.7, v0 0.04,
+    S0 100, r 0.02, T 1; M 4, 4 steps on level 0, L <= 8, R 16, eps 1e-3) with a lookback and a
+    down-and-out call (K 100, B 80; FP64 oracle MLQMC at eps 5e-4), and the pathwise adjoint on
+    the 64 x 32 local-vol grid (Asian call, T 2, 512 steps, 16 x 2^18 scrambled paths, price +
+    delta + rho + 2048 node vegas; FP64 oracle price and central differences)."""
     out = {}
 
     def timed(fn):
@@ -157,37 +194,87 @@ def configs_bench(eng):
 
     m, p = eng.gbm(100.0, 0.05, 0.2, 1.0), eng.european(100.0, 0.05, 1.0)
     r, t = timed(lambda: eng.run_mc(m, p, 1e-2, 64, eng.mc_cfg(pilot_n=1 << 14)))
+    o = orv.get("mc_gbm_european", {})
     out["mc_gbm_european"] = {"price": r["price"], "std_error": r["std_error"], "time_s": t,
-                              "path_steps_per_s": r["path_steps"] / t}
+                              "path_steps_per_s": r["path_steps"] / t,
+                              "vs_oracle": vs_oracle(r["price"], r["std_error"], o.get("value"), 0.0, o.get("kind", ""))}
     h = eng.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)
     for name, pay in (("lookback", eng.lookback(0.2)), ("down_out", eng.barrier_down_out(100.0, 80.0, 0.2, 0.02, 1.0))):
         r, t = timed(lambda: eng.run_mlqmc(h, pay, 1e-3, eng.mlmc_cfg(M=4, n0_steps=4, max_L=8,
                                                                      flags=eng.FLAG_HESTON_MILSTEIN),
                                            eng.qmc_cfg(R=16)))
+        o = orv.get("mlqmc_heston_" + name, {})
         out["mlqmc_heston_" + name] = {"price": r["price"], "std_error": r["std_error"], "levels": r["levels"],
-                                       "time_s": t, "path_steps_per_s": r["path_steps"] / t}
+                                       "converged": bool(r["converged"]), "time_s": t,
+                                       "path_steps_per_s": r["path_steps"] / t,
+                                       "vs_oracle": vs_oracle(r["price"], r["std_error"], o.get("value"), o.get("se", 0.0),
+                                                              o.get("kind", ""))}
     K, tt, grid = eng.config4_surface()
     lv = eng.localvol_grid(K, tt, grid, 100.0, 0.05, 2.0)
     (g, _), t = timed(lambda: eng.adjoint(lv, eng.asian(100.0), 512, salt_base=42, R=16, n_points=1 << 18))
-    out["adjoint_localvol_asian"] = {"price": g["price"], "delta": g["delta"], "rho": g["rho"], "vega": g["vega"],
-                                     "time_s": t, "path_steps_per_s": g["path_steps"] / t,
-                                     "paths_per_s": g["n_paths"] / t}
+    o = orv.get("adjoint_localvol_asian", {})
+    greeks = {}
+    for k in ("delta", "rho", "vega"):
+        if k in o:
+            greeks[k] = {"oracle_fd": o[k], "error": g[k] - o[k], "rel_error": (g[k] - o[k]) / abs(o[k])}
+    out["adjoint_localvol_asian"] = {"price": g["price"], "price_se": g["price_se"], "delta": g["delta"], "rho": g["rho"],
+                                     "vega": g["vega"], "time_s": t, "path_steps_per_s": g["path_steps"] / t,
+                                     "paths_per_s": g["n_paths"] / t,
+                                     "vs_oracle": vs_oracle(g["price"], g["price_se"], o.get("price"),
+                                                            o.get("price_se", 0.0), o.get("kind", "")),
+                                     "greeks_vs_oracle_fd": greeks or None}
     return out
 
 
-def book_bench(eng, n):
+def book_checks(eng, opts, res, orv, first_index=0):
+    """Convergence counts and FP64-oracle errors of one book run: options whose bias test passed,
+    options whose standard error reached their eps, one-asset options against Black–Scholes (their
+    basket is the asset itself), and the sampled multi-asset options against the FP64 oracle's
+    MLQMC values."""
+    import numpy as np
+    conv = sum(1 for x in res if x["converged"])
+    se_ok = sum(1 for o, x in zip(opts, res) if x["std_error"] <= o.eps)
+    one = []
+    for o, x in zip(opts, res):
+        if o.n_assets == 1:
+            ref = bs_call(float(o.S0[0]), o.K, o.T, o.r, float(o.sigma[0]))
+            one.append((x["price"] - ref, x["std_error"], o.eps, x["converged"]))
+    out = {"options": len(opts), "converged": conv, "se_le_eps": se_ok}
+    if one:
+        e = np.array([a for a, _, _, _ in one])
+        z = np.array([abs(a) / b if b > 0 else 0.0 for a, b, _, _ in one])
+        ok = sum(1 for a, b, ep, c in one if abs(a) <= ep / math.sqrt(2.0) + 3 * b)
+        out["one_asset_vs_black_scholes"] = {
+            "n": len(one), "max_abs_error": float(np.abs(e).max()), "mean_abs_error": float(np.abs(e).mean()),
+            "median_abs_error_in_se": float(np.median(z)),
+            "within_bias_bound_plus_3se": ok,
+            "note": "error = MLQMC price - Black-Scholes; the MLQMC estimate targets the finest level's Euler "
+                    "price, whose bias the stopping test bounds by eps/sqrt(2) when the option converged"}
+    samp = orv.get("book", {}).get("options", {})
+    rows = []
+    for k, v in samp.items():
+        i = int(k) - first_index
+        if 0 <= i < len(res):
+            rows.append({"option": int(k), "assets": v.get("assets"),
+                         **vs_oracle(res[i]["price"], res[i]["std_error"], v["value"], v.get("se", 0.0),
+                                     orv["book"].get("kind", ""))})
+    if rows:
+        out["sample_vs_fp64_oracle"] = rows
+    return out
+
+
+def book_bench(eng, n, n_loose, orv):
     """The batched heterogeneous book against its plain form on the same GPU: the first n options
     of the 4096-option synthetic book (d ~ U{1..16}, correlated GBM, Dirichlet weights, T ~
     U[0.1, 3], 16-512 finest steps, eps ~ U[5e-4, 5e-3]), each priced by MLQMC (R = 16, M = 2)
-    with its per-asset pathwise deltas.  Each mode is timed by the library around its pricing
-    loop (host wall time with the device synchronised), after a warm-up book.  Under torchrun
-    the options are dealt round-robin over the ranks (the same n in total) and the time is the
-    maximum over ranks."""
+    with its per-asset pathwise deltas: at each option's own eps, at the metric's eps = 1e-3 for
+    every option, and (the first n_loose options) at the loosest eps of the range, 5e-3.  Each mode
+    is timed by the library around its pricing loop (host wall time with the device
+    synchronised), after a warm-up book.  Under torchrun the options are dealt round-robin over the
+    ranks (the same n in total) and the time is the maximum over ranks."""
     import torch
     rank, _, world = dist_env()
     book = eng.config5_book(n=4096, seed=5)
-    full = book[:n]
-    mine = [full[i] for i in range(rank, n, world)]
     # warm-up: one option of every basket width (all kernels loaded, graphs and streams set up)
     warm = []
     for d in range(1, 17):
@@ -197,7 +284,8 @@ def book_bench(eng, n):
         warm.append(c)
     eng.book_price(warm, eng.BOOK_BATCHED)
     eng.book_price(warm, eng.BOOK_PLAIN)
-    def both_modes(opts):
+
+    def both_modes(opts, total):
         d, res = {}, {}
         for name, mode in (("batched", eng.BOOK_BATCHED), ("plain", eng.BOOK_PLAIN)):
             r, st = eng.book_price(opts, mode) if opts else ([], {"time_s": 0.0, "rounds": 0, "launches": 0,
@@ -211,34 +299,33 @@ def book_bench(eng, n):
                 torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
                 agg = torch.cat([t, w])
             tmax, normals, psteps = agg.tolist()
-            d[name] = {"options_per_s": n / tmax, "time_s": tmax, "rounds": st["rounds"],
+            d[name] = {"options_per_s": total / tmax, "time_s": tmax, "rounds": st["rounds"],
                        "launches": st["launches"], "normals_per_s": normals / tmax,
                        "path_steps_per_s": psteps / tmax}
         d["batched_over_plain"] = d["batched"]["options_per_s"] / d["plain"]["options_per_s"]
         d["bit_identical"] = all(a["price"] == b["price"] and bool((a["delta"] == b["delta"]).all())
                                  for a, b in zip(res["batched"], res["plain"]))
+        d["checks"] = book_checks(eng, opts, res["batched"], orv) if world == 1 else None
         d["converged"] = sum(1 for x in res["batched"] if x["converged"])
         return d
 
-    out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5); "
-                                     "MLQMC R=16 M=2 n0=1, per-option eps, price + per-asset delta" % n,
+    def at_eps(opts, eps):
+        out = []
+        for o in opts:
+            c = type(o).from_buffer_copy(o)   # copies; the arrays stay with `book`
+            c.eps = eps
+            out.append(c)
+        return out
+
+    mine = [book[i] for i in range(rank, n, world)]
+    out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5), %.1f %% of it; "
+                                     "MLQMC R=16 M=2 n0=1, price + per-asset delta" % (n, 100.0 * n / 4096),
            "sharding": "options round-robin over %d rank(s), fixed total" % world}
-    out.update(both_modes(mine))
-    # the same options at the metric's eps = 1e-3 each (copies; the arrays stay with `book`)
-    at = []
-    for o in mine:
-        c = type(o).from_buffer_copy(o)
-        c.eps = 1e-3
-        at.append(c)
-    out["eps_1e-3"] = both_modes(at)
-    # and at the loosest eps of the book's range, 5e-3: cheap options, where the plain form's
-    # per-level launches and synchronisations weigh most
-    loose = []
-    for o in mine:
-        c = type(o).from_buffer_copy(o)
-        c.eps = 5e-3
-        loose.append(c)
-    out["eps_5e-3"] = both_modes(loose)
+    out["eps_1e-3"] = both_modes(at_eps(mine, 1e-3), n)
+    out["own_eps"] = both_modes(mine, n)
+    loose = [book[i] for i in range(rank, n_loose, world)]
+    out["eps_5e-3"] = both_modes(at_eps(loose, 5e-3), n_loose)
+    out["eps_5e-3"]["options"] = n_loose
     return out
 
 
@@ -308,8 +395,10 @@ def main():
     ap.add_argument("--e2e-runs", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true", help="skip the bridge / PCA orderings")
-    ap.add_argument("--book-options", type=int, default=64,
+    ap.add_argument("--book-options", type=int, default=256,
                     help="options of the synthetic basket book priced batched and plain (0: skip)")
+    ap.add_argument("--book-options-loose", type=int, default=4096,
+                    help="options priced at the loosest eps of the range (5e-3)")
     ap.add_argument("--no-configs", action="store_true", help="skip the MC / Heston MLQMC / adjoint workloads")
     ap.add_argument("--book-slice", default=None, metavar="D:LEVEL[:POINTS]",
                     help="only price one slice of a D-asset basket at LEVEL through the book kernel "
@@ -380,7 +469,9 @@ def main():
     ps_per_step = REPS * N * STEPS
     value = world * ps_per_step * args.steps / (total_ms * 1e-3)
     chk = sums.cpu().numpy().reshape(REPS, 2)
-    price = float((chk[:, 0] / N).mean())
+    rmeans = chk[:, 0] / N
+    price = float(rmeans.mean())
+    price_se = float(rmeans.std(ddof=1) / math.sqrt(REPS))
 
     # the same workload under Brownian-bridge and PCA (tcgen05) ordering, same timing rules
     variants = {}
@@ -402,9 +493,17 @@ def main():
                 b_.synchronize()
                 tv += a_.elapsed_time(b_)
             nv = max(3, args.steps // 2)
+            vm = sums.cpu().numpy().reshape(REPS, 2)[:, 0] / N
             variants[name] = {"value": ps_per_step * nv / (tv * 1e-3), "ms_per_step": tv / nv,
-                              "price": float((sums.cpu().numpy().reshape(REPS, 2)[:, 0] / N).mean())}
+                              "price": float(vm.mean()), "std_error": float(vm.std(ddof=1) / math.sqrt(REPS))}
             h.close()
+
+    # the same workload with the geometric-average payoff, against its discrete closed form
+    eng.qmc_pass_device(m, eng.geom_asian(K), STEPS, sums.data_ptr(), sp, salt_base=salt, R=REPS, offset=0,
+                        n_points=N)
+    torch.cuda.synchronize()
+    gm = sums.cpu().numpy().reshape(REPS, 2)[:, 0] / N
+    geom_check = {"price": float(gm.mean()), "std_error": float(gm.std(ddof=1) / math.sqrt(REPS))}
 
     # e2e: the reference-facing adaptive driver with host structs
     cfg = eng.qmc_cfg(R=REPS, N0_per_replica=1 << 14, salt_base=salt)
@@ -426,8 +525,9 @@ def main():
     import ctypes
     h2d_e2e = ctypes.sizeof(m) + ctypes.sizeof(p) + ctypes.sizeof(cfg)
 
-    book = None if args.book_options <= 0 else book_bench(eng, args.book_options)
-    others = None if args.no_configs else configs_bench(eng)
+    orv = oracle_values()
+    book = None if args.book_options <= 0 else book_bench(eng, args.book_options, args.book_options_loose, orv)
+    others = None if args.no_configs else configs_bench(eng, orv)
 
     if world > 1:
         import torch.distributed as dist
@@ -459,7 +559,17 @@ def main():
                    "seq_len": STEPS, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed (256 MiB write) between steps; inputs are parameter-sized"},
         "price_check": price,
-        "orderings": variants,
+        "price_check_se": price_se,
+        "vs_oracle": vs_oracle(price, price_se, orv.get("asian_gbm_256", {}).get("value"),
+                               orv.get("asian_gbm_256", {}).get("se", 0.0), orv.get("asian_gbm_256", {}).get("kind", "")),
+        "geom_check": dict(geom_check, vs_closed_form=vs_oracle(
+            geom_check["price"], geom_check["std_error"], orv.get("asian_gbm_256", {}).get("geom_closed_form"), 0.0,
+            "discrete geometric-Asian closed form (256 monitoring dates); includes the Euler scheme's bias")),
+        "orderings": {k: dict(v, vs_oracle=vs_oracle(v["price"], v["std_error"],
+                                                     orv.get("asian_gbm_256", {}).get("value"),
+                                                     orv.get("asian_gbm_256", {}).get("se", 0.0),
+                                                     orv.get("asian_gbm_256", {}).get("kind", "")))
+                      for k, v in variants.items()},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d_e2e,
                 "d2h_bytes_per_step": doublings * REPS * 2 * 8,
                 "what": "mcq_run_qmc (run_qmc_cuda entry) eps=1e-3 from 2^14 pts/replica, host wall time; a step "
@@ -467,16 +577,26 @@ def main():
                         "the device as kernel parameters, counted in h2d), its outputs the per-replica sums of "
                         "each doubling read back (d2h)",
                 "price": e2e_last["price"], "std_error": e2e_last["std_error"], "n_samples": e2e_last["n_samples"],
+                "converged": bool(e2e_last["converged"]),
+                "vs_oracle": vs_oracle(e2e_last["price"], e2e_last["std_error"],
+                                       orv.get("asian_gbm_256", {}).get("value"), orv.get("asian_gbm_256", {}).get("se", 0.0),
+                                       orv.get("asian_gbm_256", {}).get("kind", "")),
                 "path_steps_per_run": e2e_last["path_steps"], "ms_per_run": 1e3 * e2e_t / args.e2e_runs},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                      "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": f"derived: {sm_count} SMs x 128 FP32 lanes x 2 x {mhz:.0f} MHz (median SM clock "
                                     "sampled under load); MEASURED_PEAKS.json has no FP32 figure",
-                     "flops_per_path_step": FLOPS_PER_PATH_STEP, "kernel": "k_pass<Sobol, raw, PathC<GBM, Asian>>",
+                     "flops_per_path_step": FLOPS_PER_PATH_STEP, "sfu_per_path_step": SFU_PER_PATH_STEP,
+                     "kernel": "k_pass<Sobol, raw, PathC<GBM, Asian>>",
+                     "issue_model": {"flops_per_path_step": ISSUE_MODEL_FLOPS_PER_PATH_STEP,
+                                     "achieved": achieved * ISSUE_MODEL_FLOPS_PER_PATH_STEP / FLOPS_PER_PATH_STEP,
+                                     "frac": achieved * ISSUE_MODEL_FLOPS_PER_PATH_STEP / FLOPS_PER_PATH_STEP / peak_fp32,
+                                     "what": "the inverse normal counted as the 29-flop AS241 rational"},
                      "issue_active_ncu": issue,
-                     "note": "instruction-issue bound: in the committed ncu capture the schedulers issue on "
-                             "84% of cycles, with the FMA pipe 38%, ALU 53% and MUFU 23% busy (Sobol gray-code "
-                             "integer work, conversions and the inverse normal share the issue slots)"},
+                     "note": "instruction-issue bound: the algorithmic count is 13 FP32 flops and one inverse "
+                             "normal per path-step, the kernel issues about 49 thread instructions per path-step "
+                             "(Sobol gray-code integer work, conversions, the inverse normal's own instructions, "
+                             "transposes) at the issue activity of the committed ncu capture"},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
     }
