@@ -361,6 +361,25 @@ def book_slice(spec):
                                      "normals": normals, "seconds": best, "normals_per_s": normals / best}}))
 
 
+def adjoint_case(n_points, repeats=3):
+    """The config-4 adjoint (64 x 32 local-vol grid, Asian call, T 2, 512 steps, 16 replicas x
+    n_points scrambled paths, price + delta + rho + 2048 node vegas), `repeats` calls through the
+    public API: the profiling case of k_adjoint."""
+    import torch
+    eng = load_engine()
+    eng.init(0)
+    K, tt, grid = eng.config4_surface()
+    lv = eng.localvol_grid(K, tt, grid, 100.0, 0.05, 2.0)
+    best = float("inf")
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g, _ = eng.adjoint(lv, eng.asian(100.0), 512, salt_base=42, R=16, n_points=n_points)
+        best = min(best, time.perf_counter() - t0)
+    print(json.dumps({"adjoint_case": {"paths": 16 * n_points, "seconds": best, "price": g["price"],
+                                       "delta": g["delta"], "rho": g["rho"], "vega": g["vega"]}}))
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
@@ -403,8 +422,13 @@ def main():
     ap.add_argument("--book-slice", default=None, metavar="D:LEVEL[:POINTS]",
                     help="only price one slice of a D-asset basket at LEVEL through the book kernel "
                          "(R = 16, M = 2, n0 = 1) and print its normals/s: the profiling case")
+    ap.add_argument("--adjoint-case", type=int, default=None, metavar="POINTS",
+                    help="only run the config-4 local-vol adjoint with 16 x POINTS paths, three times (the "
+                         "profiling case of k_adjoint)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.adjoint_case:
+        return adjoint_case(args.adjoint_case)
     if args.impl == "reference":
         return run_reference(args)
     if args.book_slice:

@@ -484,15 +484,28 @@ constexpr int kIterCap = 50;   // run_mlqmc_cuda's iteration cap (:1950)
 
 size_t book_smem(int cls) { return (size_t)kWarpsPerBlock * book_warp_floats(cls) * sizeof(float); }
 
-// Resident CTAs per SM each width class is compiled for (its register budget).
+// Resident CTAs per SM each width class is compiled for (its register budget): two launch
+// variants per class, the measured default and one more CTA per SM (d 1-4: one fewer), which
+// differ only in register allocation; the autotuner keeps the faster per class.
 using BookFn = void (*)(BookArgs);
-BookFn book_fn(int cls) {
-    switch (cls) {
+constexpr int kBookVariants = 2;
+BookFn book_fn(int cls, int variant) {
+    switch (cls * kBookVariants + variant) {
         case 0: return k_book<0, 4>;
-        case 1: return k_book<1, 2>;
-        case 2: return k_book<2, 2>;
-        default: return k_book<3, 2>;
+        case 1: return k_book<0, 3>;
+        case 2: return k_book<1, 2>;
+        case 3: return k_book<1, 3>;
+        case 4: return k_book<2, 2>;
+        case 5: return k_book<2, 3>;
+        case 6: return k_book<3, 2>;
+        default: return k_book<3, 3>;
     }
+}
+inline uint64_t book_tune_key(int cls) { return (2ULL << 40) | (uint64_t)cls; }
+// the variant the tuner has settled on for a class (0 while it is still trying)
+inline int book_variant(int cls) {
+    const TuneState* ts = tune_state(book_tune_key(cls));
+    return (ts && ts->chosen >= 0) ? ts->chosen : 0;
 }
 
 struct OptState {
@@ -741,22 +754,32 @@ struct BookRunner {
         return chunk;
     }
 
-    static int grid_of(int cls) {
-        static int per_sm[kBookClasses] = {-1, -1, -1, -1};
-        if (per_sm[cls] < 0) {
-            const void* fn = (const void*)book_fn(cls);
+    static int grid_of(int cls, int variant) {
+        static int per_sm[kBookClasses][kBookVariants] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
+        if (per_sm[cls][variant] < 0) {
+            const void* fn = (const void*)book_fn(cls, variant);
             MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)book_smem(cls)));
             int b = 0;
             MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, book_smem(cls)));
             MCQ_REQUIRE(b > 0, MCQ_ERR_INTERNAL, "book kernel does not fit on an SM");
-            per_sm[cls] = b;
+            per_sm[cls][variant] = b;
         }
-        return per_sm[cls] * engine().sm_count;
+        return per_sm[cls][variant] * engine().sm_count;
     }
 
-    void launch_book(int cls, const BookArgs& a, int grid, cudaStream_t st_) {
+    void launch_book(int cls, int variant, const BookArgs& a, int grid, cudaStream_t st_) {
         void* argv[] = {(void*)&a};
-        MCQ_CUDA(cudaLaunchKernel((const void*)book_fn(cls), dim3(grid), dim3(kThreads), argv, book_smem(cls), st_));
+        MCQ_CUDA(cudaLaunchKernel((const void*)book_fn(cls, variant), dim3(grid), dim3(kThreads), argv,
+                                 book_smem(cls), st_));
+    }
+    // a per-slice launch of one class: the tuner's pick, timed while it is still trying variants
+    void launch_book_tuned(int cls, const BookArgs& a, int chunks, double normals, cudaStream_t st_) {
+        TuneState* trial = nullptr;
+        const int v = tune_pick(book_tune_key(cls), kBookVariants, normals, (double)(1 << 26), &trial);
+        const int grid = std::max(1, std::min(grid_of(cls, v), (chunks + kWarpsPerBlock - 1) / kWarpsPerBlock));
+        if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[v][0], st_));
+        launch_book(cls, v, a, grid, st_);
+        if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[v][1], st_));
     }
     void launch_fin(const BookArgs& a, int grid, cudaStream_t st_) {
         void* argv[] = {(void*)&a};
@@ -775,8 +798,7 @@ struct BookRunner {
         for (auto& e : join) MCQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         cudaGraphExec_t exec = nullptr;
         const void* captured_records = nullptr;
-        int grid[kBookClasses];
-        for (int c = 0; c < kBookClasses; c++) grid[c] = grid_of(c);
+        int grid[kBookClasses], var[kBookClasses];
         std::vector<BookSpec> sp;
         auto cleanup = [&]() {
             if (exec) cudaGraphExecDestroy(exec);
@@ -795,15 +817,22 @@ struct BookRunner {
                 for (auto& x : sp) chunks += (long long)R * x.cpr;
                 grow(s.records, sizeof(double) * kBookNST * (size_t)std::max<long long>(chunks, 1));
                 upload(s, sp);
-                if (!exec || captured_records != s.records.p) {   // (re)capture when a buffer moved
+                bool var_changed = false;
+                for (int c = 0; c < kBookClasses; c++) var_changed |= exec && var[c] != book_variant(c);
+                // (re)capture when a buffer moved or the tuner settled a class on another variant
+                if (!exec || captured_records != s.records.p || var_changed) {
                     if (exec) { MCQ_CUDA(cudaGraphExecDestroy(exec)); exec = nullptr; }
+                    for (int c = 0; c < kBookClasses; c++) {
+                        var[c] = book_variant(c);
+                        grid[c] = grid_of(c, var[c]);
+                    }
                     const BookArgs a = args(s);
                     cudaGraph_t g = nullptr;
                     MCQ_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
                     MCQ_CUDA(cudaEventRecord(fork, s.stream));
                     for (int c = 0; c < kSide; c++) MCQ_CUDA(cudaStreamWaitEvent(side[c], fork, 0));
-                    for (int c = kBookClasses - 1; c >= 1; c--) launch_book(c, a, grid[c], side[c - 1]);
-                    launch_book(0, a, grid[0], s.stream);
+                    for (int c = kBookClasses - 1; c >= 1; c--) launch_book(c, var[c], a, grid[c], side[c - 1]);
+                    launch_book(0, var[0], a, grid[0], s.stream);
                     for (int c = 0; c < kSide; c++) {
                         MCQ_CUDA(cudaEventRecord(join[c], side[c]));
                         MCQ_CUDA(cudaStreamWaitEvent(s.stream, join[c], 0));
@@ -857,8 +886,9 @@ struct BookRunner {
                     grow(sl.records, sizeof(double) * kBookNST * (size_t)R * one[0].cpr);
                     const int chunks = upload(sl, one);
                     const BookArgs a = args(sl);
-                    launch_book(cls, a, std::max(1, std::min(grid_of(cls), (chunks + kWarpsPerBlock - 1) / kWarpsPerBlock)),
-                                sl.stream);
+                    launch_book_tuned(cls, a, chunks,
+                                      (double)R * (double)one[0].n_points * (double)opts[i].n_assets * (double)nfine(l),
+                                      sl.stream);
                     launch_fin(a, 1, sl.stream);
                     double* ho = (double*)sl.hout.ensure(sizeof(double) * kBookOut);
                     MCQ_CUDA(cudaMemcpyAsync(ho, a.out, sizeof(double) * kBookOut, cudaMemcpyDeviceToHost, sl.stream));
@@ -913,7 +943,8 @@ void book_level_sums(const mcq_book_option& opt, const mcq_mlmc_cfg& ml, const m
     grow(s.records, sizeof(double) * kBookNST * (size_t)b.R * one[0].cpr);
     const int chunks = b.upload(s, one);
     const int cls = book_class(opt.n_assets);
-    b.launch_book(cls, b.args(s), BookRunner::grid_of(cls), s.stream);
+    b.launch_book_tuned(cls, b.args(s), chunks, (double)b.R * (double)n_points * (double)opt.n_assets * (double)b.nfine(level),
+                        s.stream);
     std::vector<double> rec((size_t)chunks * kBookNST);
     MCQ_CUDA(cudaMemcpyAsync(rec.data(), s.records.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.stream));
     MCQ_CUDA(cudaStreamSynchronize(s.stream));

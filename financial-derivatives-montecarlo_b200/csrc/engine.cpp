@@ -325,6 +325,54 @@ KernelInfo& kernel_info(const void* fn, size_t smem) {
     return E.kinfo[fn];
 }
 
+// The autotuner.  A family of kernels compiled with nvar launch variants that differ only in
+// register allocation, scheduling or work granularity inside a launch (never in arithmetic, so
+// every variant gives the same bits) is tuned once per process: its first launches of at least
+// min_units work units run one variant each, timed with events on the launching stream (the
+// caller records them around its launch when *trial is set), and the variant with the least time
+// per unit is kept.  MCQ_TUNE=<v> forces variant v.
+int tune_pick(uint64_t key, int nvar, double units, double min_units, TuneState** trial) {
+    Engine& E = engine();
+    *trial = nullptr;
+    if (nvar <= 1) return 0;
+    if (const char* force = std::getenv("MCQ_TUNE")) return std::min(std::max(std::atoi(force), 0), nvar - 1);
+    TuneState& ts = E.tune[key];
+    for (int v = 0; v < nvar; v++) {
+        if (ts.pending[v]) {
+            float ms = 0.f;
+            MCQ_CUDA(cudaEventSynchronize(ts.ev[v][1]));
+            MCQ_CUDA(cudaEventElapsedTime(&ms, ts.ev[v][0], ts.ev[v][1]));
+            ts.per_unit[v] = ms / ts.units[v];
+            ts.pending[v] = false;
+            ts.done[v] = true;
+        }
+    }
+    int first_untried = -1;
+    for (int v = 0; v < nvar; v++)
+        if (!ts.done[v] && first_untried < 0) first_untried = v;
+    if (ts.chosen < 0 && first_untried < 0) {
+        ts.chosen = 0;
+        for (int v = 1; v < nvar; v++)
+            if (ts.per_unit[v] < ts.per_unit[ts.chosen]) ts.chosen = v;
+    }
+    if (ts.chosen >= 0) return ts.chosen;
+    if (units < min_units || ts.pending[first_untried]) return 0;
+    const int v = first_untried;
+    if (!ts.ev[v][0]) {
+        MCQ_CUDA(cudaEventCreate(&ts.ev[v][0]));
+        MCQ_CUDA(cudaEventCreate(&ts.ev[v][1]));
+    }
+    ts.units[v] = units;
+    ts.pending[v] = true;
+    *trial = &ts;
+    return v;
+}
+
+const TuneState* tune_state(uint64_t key) {
+    auto it = engine().tune.find(key);
+    return it == engine().tune.end() ? nullptr : &it->second;
+}
+
 void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     Engine& E = engine();
     MCQ_REQUIRE(a.m && a.p, MCQ_ERR_INVALID, "null model or payoff");
@@ -404,48 +452,9 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     TuneState* trial = nullptr;
     const int nvar = (a.dump || packed || assist) ? 1 : n_variants(a.gen, knoise, a.est, k.model);
     if (nvar > 1) {
-        const char* force = std::getenv("MCQ_TUNE");
-        if (force) {
-            variant = std::min(std::max(std::atoi(force), 0), nvar - 1);
-        } else {
-            const uint64_t key = (uint64_t)a.gen | ((uint64_t)knoise << 4) | ((uint64_t)a.est << 8) |
-                                 ((uint64_t)k.model << 12) | ((uint64_t)a.p->kind << 16);
-            TuneState& ts = E.tune[key];
-            for (int v = 0; v < nvar; v++) {
-                if (ts.pending[v]) {
-                    float ms = 0.f;
-                    MCQ_CUDA(cudaEventSynchronize(ts.ev[v][1]));
-                    MCQ_CUDA(cudaEventElapsedTime(&ms, ts.ev[v][0], ts.ev[v][1]));
-                    ts.per_unit[v] = ms / ts.units[v];
-                    ts.pending[v] = false;
-                    ts.done[v] = true;
-                }
-            }
-            int first_untried = -1;
-            for (int v = 0; v < nvar; v++)
-                if (!ts.done[v] && first_untried < 0) first_untried = v;
-            if (ts.chosen < 0 && first_untried < 0) {
-                ts.chosen = 0;
-                for (int v = 1; v < nvar; v++)
-                    if (ts.per_unit[v] < ts.per_unit[ts.chosen]) ts.chosen = v;
-            }
-            const double units = (double)a.R * (double)a.n_points * (double)k.D;
-            if (ts.chosen >= 0) {
-                variant = ts.chosen;
-            } else if (units >= (double)(1 << 26)) {
-                const int v = first_untried;
-                if (!ts.pending[v]) {
-                    if (!ts.ev[v][0]) {
-                        MCQ_CUDA(cudaEventCreate(&ts.ev[v][0]));
-                        MCQ_CUDA(cudaEventCreate(&ts.ev[v][1]));
-                    }
-                    variant = v;
-                    ts.units[v] = units;
-                    ts.pending[v] = true;
-                    trial = &ts;
-                }
-            }
-        }
+        const uint64_t key = (uint64_t)a.gen | ((uint64_t)knoise << 4) | ((uint64_t)a.est << 8) |
+                             ((uint64_t)k.model << 12) | ((uint64_t)a.p->kind << 16);
+        variant = tune_pick(key, nvar, (double)a.R * (double)a.n_points * (double)k.D, (double)(1 << 26), &trial);
         if (variant > 0) fn = lookup_variant(a.gen, knoise, a.est, k.model, a.p->kind, variant);
     }
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED,
@@ -630,7 +639,14 @@ void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t 
     fill_params(ws, a, k);
     const int n_nodes = (m.kind == MCQ_MODEL_LOCALVOL_GRID) ? m.lv_nK * m.lv_nt : 0;
     MCQ_REQUIRE(n_nodes <= 4096, MCQ_ERR_UNSUPPORTED, "adjoint Greeks: at most 4096 grid nodes");
-    const void* fn = lookup_adjoint(k.model, p.kind);
+    // the checkpoint interval is a launch variant (same bits); variants whose shared memory does
+    // not fit one CTA per SM are left out
+    int nvar = adjoint_variants(k.model);
+    while (nvar > 1 && adjoint_smem_bytes(k.model, n_steps, n_nodes, nvar - 1) > 227 * 1024) nvar--;
+    TuneState* trial = nullptr;
+    const uint64_t key = (1ULL << 40) | ((uint64_t)k.model << 4) | (uint64_t)p.kind;
+    const int variant = tune_pick(key, nvar, (double)R * (double)n_points * (double)n_steps, (double)(1 << 26), &trial);
+    const void* fn = lookup_adjoint(k.model, p.kind, variant);
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no adjoint kernel for this model / payoff");
     const uint64_t g0 = offset >> 5;
     const uint64_t G = ((offset + n_points - 1) >> 5) - g0 + 1;
@@ -655,14 +671,16 @@ void adjoint_run(const mcq_model& m, const mcq_payoff& p, int n_steps, uint32_t 
         MCQ_CUDA(cudaMemsetAsync(d_nodes, 0, sizeof(double) * n_nodes, ws.stream));
     }
     k.node_out = d_nodes;
-    const size_t smem = adjoint_smem_bytes(k.model, n_steps, n_nodes);
+    const size_t smem = adjoint_smem_bytes(k.model, n_steps, n_nodes, variant);
     KernelInfo& ki = kernel_info(fn, smem);
     long long blocks = std::min<long long>(((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock,
                                            (long long)ki.blocks_per_sm * E.sm_count);
     blocks = std::max<long long>(blocks, 1);
     double* d_out = (double*)ws.sums.ensure(sizeof(double) * (size_t)R * 4);
     void* args[] = {&k};
+    if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[variant][0], ws.stream));
     MCQ_CUDA(cudaLaunchKernel(fn, dim3((unsigned)blocks), dim3(kThreads), args, smem, ws.stream));
+    if (trial) MCQ_CUDA(cudaEventRecord(trial->ev[variant][1], ws.stream));
     launch_finalize(k.partials, R, k.items_per_rep, 4, d_out, ws.stream);
     E.launches += 2;
     MCQ_CUDA(cudaGetLastError());

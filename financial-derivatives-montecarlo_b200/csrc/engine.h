@@ -105,6 +105,11 @@ struct TuneState {
     cudaEvent_t ev[kMaxVariants][2] = {};
 };
 
+// Autotuner: the launch variant of family `key` (nvar variants) for a launch of `units` work;
+// *trial set: record ev[variant][0] / [1] around the launch (engine.cpp).
+int tune_pick(uint64_t key, int nvar, double units, double min_units, TuneState** trial);
+const TuneState* tune_state(uint64_t key);   // nullptr until the family has been launched
+
 struct Engine {
     std::mutex mu;
     bool ready = false;

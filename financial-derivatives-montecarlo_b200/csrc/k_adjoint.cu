@@ -2,15 +2,17 @@
 // reference, which computes no sensitivities).
 //
 // For each path (lane) the forward sweep steps S_k -> S_{k+1} = S_k (1 + mu h + sigma_k dW_k),
-// keeps the payoff state and checkpoints S every 16 steps in shared memory.  The reverse sweep
-// walks the 32-step Sobol tiles backwards: it regenerates the tile's normals (same warp-
-// transposed generator as the pricing pass), recomputes each 16-step segment from its
-// checkpoint, and propagates
+// keeps the payoff state and checkpoints S every CK steps (16, 32 or 8: an autotuned launch
+// variant) in shared memory.  The reverse sweep walks the 32-step Sobol tiles backwards: it
+// regenerates the tile's normals (same warp-transposed generator as the pricing pass), recomputes
+// each CK-step segment from its checkpoint, and propagates
 //     Sbar_k = Sbar_{k+1} dS_{k+1}/dS_k + dP/dS_k,
 //     mubar += Sbar_{k+1} S_k h,            sigmabar += Sbar_{k+1} dS_{k+1}/dsigma,
 // and, for the grid local-vol model, adds Sbar_{k+1} S_k dW_k w_n to the four bilinear nodes n of
-// (S_k, t_k) in an FP64 shared-memory array per CTA (summed per lane over the consecutive steps
-// that stay in one grid cell, then added with one atomic per node).  Payoffs are the Lipschitz ones:
+// (S_k, t_k) in an FP32 shared-memory array per CTA (summed per lane over the consecutive steps
+// that stay in one grid cell, then added with one native float atomic per node; a path changes
+// cell about once a step on the benchmark's grid, and the FP64 shared atomics this replaced were
+// the kernel's top stall), whose totals go to the FP64 output once per CTA.  Payoffs are the Lipschitz ones:
 // European (discounted), arithmetic Asian and floating-strike lookback (BGK factor constant).
 // Per path it yields P, delta = Sbar_0 (plus, for the parametric Dupire model, whose volatility
 // (S/S0)^(beta-1) is scaled by S0, the sensitivity through that scale, so that delta is the
@@ -22,7 +24,9 @@
 
 namespace mcq {
 
-constexpr int kCk = 16;   // checkpoint interval (steps)
+// Checkpoint interval CK (steps): 16 by default; the autotuner also tries 32 and 8 (a launch
+// variant: more or fewer recomputed steps per checkpoint, the same arithmetic and the same bits).
+constexpr int kCkVariants[3] = {16, 32, 8};
 
 struct LvEval {
     float sig, dsig;
@@ -76,21 +80,22 @@ __device__ __forceinline__ float local_sigma(const KParams& p, float S, float t,
     }
 }
 
-template <int MOD, int PAY>
+template <int MOD, int PAY, int CK>
 __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__ KParams p) {
+    constexpr int kCk = CK;
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int N = p.n_steps;
     const int n_ck = N / kCk + 1;
     const int per_warp = 1024 + n_ck * 32 + kCk * 32;
-    double* nodes = reinterpret_cast<double*>(smem4);             // [n_nodes] FP64, CTA-wide
-    const int node_doubles = (MOD == MOD_LVGRID) ? ((p.lv_nK * p.lv_nt + 1) & ~1) : 0;
-    float* wbase = reinterpret_cast<float*>(nodes + node_doubles) + wib * per_warp;
+    float* nodes = reinterpret_cast<float*>(smem4);               // [n_nodes] FP32, CTA-wide
+    const int node_floats = (MOD == MOD_LVGRID) ? ((p.lv_nK * p.lv_nt + 3) & ~3) : 0;
+    float* wbase = nodes + node_floats + wib * per_warp;
     float* buf = wbase;               // 32 x 32 transpose tile
     float* ck = wbase + 1024;         // checkpoints [n_ck][32]
-    float* seg = ck + n_ck * 32;      // recomputed segment [16][32]
+    float* seg = ck + n_ck * 32;      // recomputed segment [CK][32]
     if constexpr (MOD == MOD_LVGRID) {
-        for (int i = threadIdx.x; i < node_doubles; i += blockDim.x) nodes[i] = 0.0;
+        for (int i = threadIdx.x; i < node_floats; i += blockDim.x) nodes[i] = 0.f;
         __syncthreads();
     }
     const float h = p.h, sqh = p.sqrt_h, muh = p.mu * p.h;
@@ -158,13 +163,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             // grid local vol: the node sensitivities of consecutive steps in the same cell are
             // summed in registers (FP64) and added to the CTA's node array when the cell changes
             int vcell = -1;
-            double v00 = 0.0, v01 = 0.0, v10 = 0.0, v11 = 0.0;
+            float v00 = 0.f, v01 = 0.f, v10 = 0.f, v11 = 0.f;
             for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
                 sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
                 __syncwarp();
                 const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
 #pragma unroll 1
-                for (int s = 1; s >= 0; s--) {
+                for (int s = 32 / kCk - 1; s >= 0; s--) {
                     const int k0 = d0 + s * kCk;
                     float Sr = ck[(k0 / kCk) * 32 + lane];
 #pragma unroll 1
@@ -210,12 +215,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                                             atomicAdd(&nodes[vcell + p.lv_nK + 1], v11);
                                         }
                                         vcell = lv.n00;
-                                        v00 = v01 = v10 = v11 = 0.0;
+                                        v00 = v01 = v10 = v11 = 0.f;
                                     }
-                                    v00 += (double)(sens * lv.w00);
-                                    v01 += (double)(sens * lv.w01);
-                                    v10 += (double)(sens * lv.w10);
-                                    v11 += (double)(sens * lv.w11);
+                                    v00 = fmaf(sens, lv.w00, v00);
+                                    v01 = fmaf(sens, lv.w01, v01);
+                                    v10 = fmaf(sens, lv.w10, v10);
+                                    v11 = fmaf(sens, lv.w11, v11);
                                 }
                             }
                             const float dS1 = 1.f + muh + sig * dw + Sk * dw * dsS;
@@ -246,7 +251,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
     if constexpr (MOD == MOD_LVGRID) {
         __syncthreads();
         for (int i = threadIdx.x; i < p.lv_nK * p.lv_nt; i += blockDim.x)
-            if (nodes[i] != 0.0) atomicAdd(p.node_out + i, nodes[i]);
+            if (nodes[i] != 0.f) atomicAdd(p.node_out + i, (double)nodes[i]);
     }
 }
 
@@ -374,21 +379,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_adjoint_heston(const __grid_con
     }
 }
 
-template <int MOD>
+template <int MOD, int CK>
 static const void* adj_payoff(int pay) {
     switch (pay) {
-        case PAY_EUR: return (const void*)&k_adjoint<MOD, PAY_EUR>;
-        case PAY_ASIAN: return (const void*)&k_adjoint<MOD, PAY_ASIAN>;
-        case PAY_LOOKBACK: return (const void*)&k_adjoint<MOD, PAY_LOOKBACK>;
+        case PAY_EUR: return (const void*)&k_adjoint<MOD, PAY_EUR, CK>;
+        case PAY_ASIAN: return (const void*)&k_adjoint<MOD, PAY_ASIAN, CK>;
+        case PAY_LOOKBACK: return (const void*)&k_adjoint<MOD, PAY_LOOKBACK, CK>;
         default: return nullptr;
     }
 }
 
-const void* lookup_adjoint(int model, int payoff) {
+template <int MOD>
+static const void* adj_ck(int pay, int variant) {
+    switch (variant) {
+        case 1: return adj_payoff<MOD, kCkVariants[1]>(pay);
+        case 2: return adj_payoff<MOD, kCkVariants[2]>(pay);
+        default: return adj_payoff<MOD, kCkVariants[0]>(pay);
+    }
+}
+
+int adjoint_variants(int model) { return model == MOD_HESTON ? 1 : 3; }
+
+const void* lookup_adjoint(int model, int payoff, int variant) {
     switch (model) {
-        case MOD_GBM: return adj_payoff<MOD_GBM>(payoff);
-        case MOD_DUPIRE: return adj_payoff<MOD_DUPIRE>(payoff);
-        case MOD_LVGRID: return adj_payoff<MOD_LVGRID>(payoff);
+        case MOD_GBM: return adj_ck<MOD_GBM>(payoff, variant);
+        case MOD_DUPIRE: return adj_ck<MOD_DUPIRE>(payoff, variant);
+        case MOD_LVGRID: return adj_ck<MOD_LVGRID>(payoff, variant);
         case MOD_HESTON:
             switch (payoff) {
                 case PAY_EUR: return (const void*)&k_adjoint_heston<PAY_EUR>;
@@ -400,14 +416,15 @@ const void* lookup_adjoint(int model, int payoff) {
     }
 }
 
-size_t adjoint_smem_bytes(int model, int n_steps, int n_nodes) {
+size_t adjoint_smem_bytes(int model, int n_steps, int n_nodes, int variant) {
     if (model == MOD_HESTON) {
         const int n_tiles = 2 * n_steps / 32;
         return (size_t)kWarpsPerBlock * (1024 + (n_tiles + 1) * 64 + 16 * 64) * sizeof(float);
     }
-    const int n_ck = n_steps / kCk + 1;
-    const size_t per_warp = (size_t)(1024 + n_ck * 32 + kCk * 32) * sizeof(float);
-    return (size_t)((n_nodes + 1) & ~1) * sizeof(double) + kWarpsPerBlock * per_warp;
+    const int ck = kCkVariants[(variant >= 0 && variant < 3) ? variant : 0];
+    const int n_ck = n_steps / ck + 1;
+    const size_t per_warp = (size_t)(1024 + n_ck * 32 + ck * 32) * sizeof(float);
+    return (size_t)((n_nodes + 3) & ~3) * sizeof(float) + kWarpsPerBlock * per_warp;
 }
 
 }  // namespace mcq

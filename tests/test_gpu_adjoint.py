@@ -210,3 +210,27 @@ def test_dupire_adjoint_vs_fp64_finite_differences(gpu, orc, pay):
                 oracle_price(orc, T.dupire(100.0, mu, s0, al, be, 1.0), T.european(100.0, mu - 1e-6, 1.0), n, 7, 1, N)) / 2e-6
     for name, ref in (("delta", delta), ("vega", vega), ("rho", rho)):
         assert abs(g[name] - ref) < 5e-4 * max(1.0, abs(ref)), (pay, name, g[name], ref)
+
+
+@pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("dupire", "eur"), ("lv", "asian"), ("gbm", "lookback")])
+def test_checkpoint_interval_variants_are_bit_identical(gpu, model, pay):
+    """The adjoint's checkpoint interval (16, 32 or 8 steps: the autotuner's launch variants) only
+    changes how many steps a reverse segment recomputes: price, delta, rho and vega are the same
+    bits under every variant, the node vegas the same up to the order of their FP32 atomics."""
+    import os
+    m = {"gbm": lambda: gpu.gbm(100.0, 0.03, 0.25, 1.0), "dupire": lambda: gpu.dupire(100.0, 0.05, 0.2, 0.5, 0.7, 1.0),
+         "lv": lambda: gpu.localvol_grid(*gpu.config4_surface(), 100.0, 0.05, 2.0)}[model]()
+    p = {"asian": gpu.asian(100.0), "eur": gpu.european(100.0, 0.05, 1.0), "lookback": gpu.lookback(0.25)}[pay]
+    out = []
+    try:
+        for v in ("0", "1", "2"):
+            os.environ["MCQ_TUNE"] = v
+            out.append(gpu.adjoint(m, p, 128, salt_base=42, R=4, n_points=8192))
+    finally:
+        os.environ.pop("MCQ_TUNE", None)
+    for g, nodes in out[1:]:
+        for k in ("price", "delta", "rho", "vega"):
+            assert g[k] == out[0][0][k], (k, g[k], out[0][0][k])
+        if nodes is not None and out[0][1] is not None:
+            # FP32 atomics: only the order of the adds differs
+            assert np.abs(nodes - out[0][1]).max() < 1e-5 * np.abs(out[0][1]).max()

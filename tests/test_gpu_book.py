@@ -242,3 +242,28 @@ def test_book_object_run_equals_book_price(gpu):
     for r, o, x in zip(ref, opts, out):
         assert r["price"] == x.price and r["std_error"] == x.std_error and r["n_samples"] == x.n_samples
         assert np.array_equal(r["delta"], np.array(x.delta[:o.n_assets]))
+
+
+def test_book_class_variants_are_bit_identical(gpu):
+    """The book's width classes under both register-budget variants (the autotuner's choices) give
+    the same prices, deltas and sample counts, batched and plain."""
+    import os
+    book = gpu.config5_book(n=4096, seed=5)
+    opts = []
+    for d in (2, 6, 10, 14):
+        o = next(o for o in book if o.n_assets == d)
+        c = type(o).from_buffer_copy(o)
+        c.eps = 10 * o.eps
+        opts.append(c)
+    res = []
+    try:
+        for v in ("0", "1"):
+            os.environ["MCQ_TUNE"] = v
+            for mode in (gpu.BOOK_BATCHED, gpu.BOOK_PLAIN):
+                res.append(gpu.book_price(opts, mode)[0])
+    finally:
+        os.environ.pop("MCQ_TUNE", None)
+    for r in res[1:]:
+        for a, b in zip(res[0], r):
+            assert a["price"] == b["price"] and a["n_samples"] == b["n_samples"]
+            assert np.array_equal(a["delta"], b["delta"])
