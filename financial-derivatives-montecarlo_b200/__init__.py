@@ -13,7 +13,7 @@ from .mcq_types import (  # noqa: F401  (re-exported builders)
     GBM, HESTON, DUPIRE, MULTI_DUPIRE, LOCALVOL_GRID, BASKET_GBM,
     EUROPEAN, ASIAN, GEOM_ASIAN, LOOKBACK, BARRIER_UP_OUT, BASKET, BARRIER_DOWN_OUT,
     RAW, BB, PCA, FLAG_COMPAT_U_INF, FLAG_COMPAT_HESTON_MLMC, FLAG_HESTON_MILSTEIN, FLAG_BASKET_OWN_S0,
-    BOOK_BATCHED, BOOK_PLAIN, book_option, config5_book,
+    BOOK_BATCHED, BOOK_PLAIN, book_option, book_single, mixed_singles, config5_book,
     gbm, heston, dupire, multi_dupire, basket_gbm, localvol_grid, config4_surface, payoff, european, asian,
     geom_asian, lookback, barrier_up_out, barrier_down_out, basket, noise_dim,
 )

@@ -37,19 +37,25 @@ constexpr int kBookNST = 4 + kMaxBasket;   // per-path statistics in a chunk rec
 constexpr int kBookOut = 2 + kMaxBasket;   // per slice: E dY, var of replica means, deltas
 constexpr int kBookMaxLevels = 12;
 constexpr int kBookMaxR = 32;
-constexpr int kBookClasses = 4;            // basket width 1-4, 5-8, 9-12, 13-16
+constexpr int kBookClasses = 5;            // basket width 1-4, 5-8, 9-12, 13-16; single-asset options
+constexpr int kSingleClass = 4;
 constexpr int kChunkNormals = 8192;        // normals per lane a chunk aims at
 constexpr int kMinChunksPerRep = 64;
 constexpr int kMaxChunksPerRep = 1024;
 
-// hdr (int32): [0] n_specs, [1] n_chunks, [2 + c] first chunk of class c, [6] = n_chunks,
-// [7 + c] first slice of class c, [11] = n_specs, [12 + c] work-queue counter of class c.
-constexpr int kHdrInts = 16;
+// hdr (int32): [0] n_specs, [1] n_chunks, [kHdrChunk0 + c] first chunk of class c (and, at
+// c = kBookClasses, n_chunks), [kHdrSlice0 + c] first slice of class c (n_specs at the end),
+// [kHdrCounter0 + c] work-queue counter of class c.
+constexpr int kHdrChunk0 = 2;
+constexpr int kHdrSlice0 = kHdrChunk0 + kBookClasses + 1;
+constexpr int kHdrCounter0 = kHdrSlice0 + kBookClasses + 1;
+constexpr int kHdrInts = kHdrCounter0 + kBookClasses;
 
 struct BookOptDev {
     double T;
     float K, disc, mu;
     int d, bsk_off, uncorrelated;
+    int kp;   // single-asset option: its level-0 parameter block in BookArgs::kps (level l at kp + l); -1: basket
 };
 
 struct BookSpec {   // one (option, level) slice: all replicas, points [offset, offset + n_points)
@@ -63,6 +69,7 @@ struct BookArgs {
     const BookSpec* specs;
     const BookOptDev* opts;
     const float* bdata;   // per option [S0 | sigma | weight | L (d x d row-major)]
+    const KParams* kps;   // single-asset options: one fused-pass parameter block per (option, level)
     const uint32_t* dirs[kBookMaxLevels];
     int dstride[kBookMaxLevels];
     int R, M, n0;
@@ -372,11 +379,11 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
     float* buf = reinterpret_cast<float*>(smem4) + wib * book_warp_floats(CLS);
     float* Ls = buf + 1024;
     double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats + kBookAssetFloats);
-    const int c_end = a.hdr[3 + CLS];
-    const int s_beg = a.hdr[7 + CLS], s_last = a.hdr[8 + CLS] - 1;
+    const int c_end = a.hdr[kHdrChunk0 + CLS + 1];
+    const int s_beg = a.hdr[kHdrSlice0 + CLS], s_last = a.hdr[kHdrSlice0 + CLS + 1] - 1;
     for (;;) {
         int c = 0;
-        if (lane == 0) c = a.hdr[2 + CLS] + atomicAdd(a.hdr + 12 + CLS, 1);
+        if (lane == 0) c = a.hdr[kHdrChunk0 + CLS] + atomicAdd(a.hdr + kHdrCounter0 + CLS, 1);
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= c_end) break;
         int lo = s_beg, hi = s_last;   // last slice of the class with chunk0 <= c
@@ -396,6 +403,78 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
             case 2: book_chunk<4 * CLS + 2>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
             case 3: book_chunk<4 * CLS + 3>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
             default: book_chunk<4 * CLS + 4>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
+        }
+    }
+}
+
+// One chunk of a single-asset option's slice: the fused pass's coupled fine / coarse consumer
+// (PathC, the pair mcq_run_mlqmc prices) on raw scrambled-Sobol normals, groups [gb, ge) of
+// replica r, with the option's parameter block for the slice's level.  Record: {dY, dY^2, Yf,
+// Yf^2} and zeros in place of the basket deltas.
+template <class C>
+__device__ __forceinline__ void single_chunk(const KParams& kp, const BookSpec& s, int r, uint64_t gb, uint64_t ge,
+                                             const uint32_t* dr, float* buf, double* rec, int lane) {
+    Acc<C::NST> acc;
+    acc.zero();
+    const uint64_t pend = (uint64_t)s.offset + s.n_points;
+    for (uint64_t h = gb; h < ge; h++) {
+        const uint64_t n = h * 32 + (uint64_t)lane;
+        C cons;
+        cons.init(kp);
+        cons.bind(r, n);
+        run_group<GEN_SOBOL, NOISE_RAW>(kp, cons, dr, 0u, h, n, buf, nullptr, lane);
+        float y[C::NST];
+        cons.finish(kp, y);
+        if (n >= s.offset && n < pend) acc.add(y);
+    }
+    acc.flush(rec, lane);
+    for (int q = C::NST + lane; q < kBookNST; q += 32) rec[q] = 0.0;
+}
+
+template <int MOD>
+__device__ __forceinline__ void single_chunk_pay(const KParams& kp, const BookSpec& s, int r, uint64_t gb,
+                                                 uint64_t ge, const uint32_t* dr, float* buf, double* rec, int lane) {
+    switch (kp.payoff) {
+        case PAY_ASIAN: single_chunk<PathC<MOD, PAY_ASIAN, true>>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+        case PAY_GEOM: single_chunk<PathC<MOD, PAY_GEOM, true>>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+        case PAY_LOOKBACK: single_chunk<PathC<MOD, PAY_LOOKBACK, true>>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+        case PAY_UPOUT: single_chunk<PathC<MOD, PAY_UPOUT, true>>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+        case PAY_DOWNOUT: single_chunk<PathC<MOD, PAY_DOWNOUT, true>>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+        default: single_chunk<PathC<MOD, PAY_EUR, true>>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+    }
+}
+
+// Persistent work-queue kernel of the single-asset class: warps take chunks of every such option and
+// level from the class's counter; each chunk runs its option's model and payoff.
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_book_single(const __grid_constant__ BookArgs a) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    float* buf = reinterpret_cast<float*>(smem4) + wib * 1024;
+    const int c_end = a.hdr[kHdrChunk0 + kSingleClass + 1];
+    const int s_beg = a.hdr[kHdrSlice0 + kSingleClass], s_last = a.hdr[kHdrSlice0 + kSingleClass + 1] - 1;
+    for (;;) {
+        int c = 0;
+        if (lane == 0) c = a.hdr[kHdrChunk0 + kSingleClass] + atomicAdd(a.hdr + kHdrCounter0 + kSingleClass, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= c_end) break;
+        int lo = s_beg, hi = s_last;   // last slice of the class with chunk0 <= c
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.specs[mid].chunk0 <= c) lo = mid; else hi = mid - 1;
+        }
+        const BookSpec s = a.specs[lo];
+        const KParams& kp = a.kps[a.opts[s.opt].kp + s.level];
+        const int q = c - s.chunk0, r = q / s.cpr, j = q - r * s.cpr;
+        const uint64_t gend = ((uint64_t)s.offset + s.n_points - 1) / 32 + 1;
+        const uint64_t gb = (s.offset >> 5) + (uint64_t)j * (uint64_t)s.gpc;
+        const uint64_t ge = min(gb + (uint64_t)s.gpc, gend);
+        const uint32_t* dr = a.dirs[s.level] + (size_t)r * 33 * (size_t)a.dstride[s.level];
+        double* rec = a.records + (size_t)c * kBookNST;
+        switch (kp.model) {
+            case MOD_HESTON: single_chunk_pay<MOD_HESTON>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+            case MOD_DUPIRE: single_chunk_pay<MOD_DUPIRE>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
+            default: single_chunk_pay<MOD_GBM>(kp, s, r, gb, ge, dr, buf, rec, lane); break;
         }
     }
 }
@@ -468,6 +547,24 @@ void book_validate(const mcq_book_option* opts, int n, const mcq_mlmc_cfg& ml, c
     for (int i = 0; i < n; i++) {
         const mcq_book_option& o = opts[i];
         const std::string tag = "book option " + std::to_string(i) + ": ";
+        if (o.model) {   // single-asset option
+            MCQ_REQUIRE(o.payoff, MCQ_ERR_INVALID, tag + "a model needs a payoff");
+            const int mk = o.model->kind, pk = o.payoff->kind;
+            MCQ_REQUIRE(mk == MCQ_MODEL_GBM || mk == MCQ_MODEL_HESTON || mk == MCQ_MODEL_DUPIRE, MCQ_ERR_UNSUPPORTED,
+                        tag + "single-asset book options take GBM, Heston or parametric Dupire models");
+            MCQ_REQUIRE(pk == MCQ_PAYOFF_EUROPEAN || pk == MCQ_PAYOFF_ASIAN || pk == MCQ_PAYOFF_GEOM_ASIAN ||
+                            pk == MCQ_PAYOFF_LOOKBACK || pk == MCQ_PAYOFF_BARRIER_UP_OUT ||
+                            pk == MCQ_PAYOFF_BARRIER_DOWN_OUT,
+                        MCQ_ERR_UNSUPPORTED, tag + "unsupported payoff for a single-asset book option");
+            MCQ_REQUIRE(o.max_L >= 2 && o.max_L < kBookMaxLevels, MCQ_ERR_INVALID, tag + "max_L must be 2..11");
+            MCQ_REQUIRE(o.eps > 0 && o.model->T > 0, MCQ_ERR_INVALID, tag + "needs eps > 0 and T > 0");
+            const long long dn = (mk == MCQ_MODEL_HESTON) ? 2 : 1;
+            long long nf = ml.n0_steps;
+            for (int l = 0; l < o.max_L && nf <= 20000; l++) nf *= ml.M;
+            MCQ_REQUIRE(nf * dn <= 20000, MCQ_ERR_RANGE,
+                        tag + "finest level x factors exceeds the 20000 Sobol dimensions of the table");
+            continue;
+        }
         MCQ_REQUIRE(o.n_assets >= 1 && o.n_assets <= kMaxBasket, MCQ_ERR_UNSUPPORTED, tag + "needs 1..16 assets");
         MCQ_REQUIRE(o.max_L >= 2 && o.max_L < kBookMaxLevels, MCQ_ERR_INVALID, tag + "max_L must be 2..11");
         MCQ_REQUIRE(o.eps > 0 && o.T > 0 && o.S0 && o.sigma, MCQ_ERR_INVALID, tag + "needs eps > 0, T > 0, S0, sigma");
@@ -482,7 +579,15 @@ namespace {
 
 constexpr int kIterCap = 50;   // run_mlqmc_cuda's iteration cap (:1950)
 
-size_t book_smem(int cls) { return (size_t)kWarpsPerBlock * book_warp_floats(cls) * sizeof(float); }
+size_t book_smem(int cls) {
+    return (size_t)kWarpsPerBlock * (cls == kSingleClass ? 1024 : book_warp_floats(cls)) * sizeof(float);
+}
+
+// normals a path of the option takes per step (assets of a basket, factors of a single-asset model)
+inline int book_width(const mcq_book_option& o) {
+    return o.model ? (o.model->kind == MCQ_MODEL_HESTON ? 2 : 1) : o.n_assets;
+}
+inline int book_class_of(const mcq_book_option& o) { return o.model ? kSingleClass : book_class(o.n_assets); }
 
 // Resident CTAs per SM each width class is compiled for (its register budget): two launch
 // variants per class, the measured default and one more CTA per SM (d 1-4: one fewer), which
@@ -498,7 +603,9 @@ BookFn book_fn(int cls, int variant) {
         case 4: return k_book<2, 2>;
         case 5: return k_book<2, 3>;
         case 6: return k_book<3, 2>;
-        default: return k_book<3, 3>;
+        case 7: return k_book<3, 3>;
+        case 8: return k_book_single<3>;
+        default: return k_book_single<4>;
     }
 }
 inline uint64_t book_tune_key(int cls) { return (2ULL << 40) | (uint64_t)cls; }
@@ -545,6 +652,7 @@ struct BookRunner {
     int R = 0, M = 0, n0 = 0, max_L_all = 2;
     DevBuf* d_opts = nullptr;     // engine scratch (workspace 0)
     DevBuf* d_bdata = nullptr;
+    DevBuf* d_kps = nullptr;      // single-asset options' parameter blocks
     std::vector<DevBuf*> dirs;    // level l's table in workspace 1 + l
     std::vector<int> dstride;
     std::vector<OptState> st;
@@ -565,6 +673,7 @@ struct BookRunner {
         a.specs = (const BookSpec*)s.specs.p;
         a.opts = (const BookOptDev*)d_opts->p;
         a.bdata = (const float*)d_bdata->p;
+        a.kps = (const KParams*)d_kps->p;
         for (int l = 0; l <= max_L_all; l++) {
             a.dirs[l] = (const uint32_t*)dirs[l]->p;
             a.dstride[l] = dstride[l];
@@ -582,12 +691,33 @@ struct BookRunner {
         R = qc.R; M = ml.M; n0 = ml.n0_steps;
         std::vector<BookOptDev> ho(n);
         std::vector<float> bd;
+        std::vector<KParams> kps;
         int dmax = 1;
         for (int i = 0; i < n; i++) {
             const mcq_book_option& o = opts[i];
+            if (o.model) {
+                // one fused-pass parameter block per level, as mcq_run_mlqmc fills it for the
+                // level's coupled pass (its table stride is the book's, set below)
+                ho[i] = BookOptDev{o.model->T, 0.f, 0.f, 0.f, book_width(o), 0, 1, (int)kps.size()};
+                for (int l = 0; l < kBookMaxLevels; l++) {
+                    KParams k{};
+                    if (l <= o.max_L) {
+                        PassArgs pa;
+                        pa.m = o.model; pa.p = o.payoff; pa.n_steps = (int)nfine(l); pa.est = EST_COUPLED;
+                        pa.M = M; pa.level0 = (l == 0); pa.mlmc_h = true; pa.R = R; pa.gen = GEN_SOBOL;
+                        pa.noise = NOISE_RAW; pa.flags = ml.flags | qc.flags;
+                        Workspace none;   // no staged arrays for these models
+                        fill_params(none, pa, k);
+                    }
+                    kps.push_back(k);
+                }
+                max_L_all = std::max(max_L_all, o.max_L);
+                dmax = std::max(dmax, book_width(o));
+                continue;
+            }
             const int d = o.n_assets;
             ho[i] = BookOptDev{o.T, (float)o.K, (float)std::exp(-o.r * o.T), (float)o.r, d, (int)bd.size(),
-                               o.L ? 0 : 1};
+                               o.L ? 0 : 1, -1};
             for (int a = 0; a < d; a++) bd.push_back((float)o.S0[a]);
             for (int a = 0; a < d; a++) bd.push_back((float)o.sigma[a]);
             for (int a = 0; a < d; a++) bd.push_back(o.weights ? (float)o.weights[a] : 1.0f / d);
@@ -599,6 +729,7 @@ struct BookRunner {
         cudaStream_t s0 = E.ws(0).stream;
         d_opts = &E.ws(0).xbuf[5];
         d_bdata = &E.ws(0).xbuf[6];
+        d_kps = &E.ws(0).xbuf[7];
         MCQ_CUDA(cudaMemcpyAsync(grow(*d_opts, sizeof(BookOptDev) * n), ho.data(), sizeof(BookOptDev) * n,
                                  cudaMemcpyHostToDevice, s0));
         MCQ_CUDA(cudaMemcpyAsync(grow(*d_bdata, sizeof(float) * bd.size()), bd.data(), sizeof(float) * bd.size(),
@@ -613,6 +744,15 @@ struct BookRunner {
             uint32_t* t = (uint32_t*)grow(*dirs[l], sizeof(uint32_t) * (size_t)R * 33 * dstride[l]);
             launch_prescramble(E.d_dv, qc.salt_base + (uint32_t)(l * R), R, dstride[l], t, s0);
         }
+        for (size_t q = 0; q < kps.size(); q++) {
+            const int l = (int)(q % kBookMaxLevels);
+            if (l <= max_L_all) kps[q].dstride = dstride[l];
+        }
+        if (!kps.empty())
+            MCQ_CUDA(cudaMemcpyAsync(grow(*d_kps, sizeof(KParams) * kps.size()), kps.data(), sizeof(KParams) * kps.size(),
+                                     cudaMemcpyHostToDevice, s0));
+        else
+            grow(*d_kps, sizeof(KParams));
         MCQ_CUDA(cudaStreamSynchronize(s0));
         max_specs = (size_t)n * (max_L_all + 1);
         st.assign(n, OptState());
@@ -708,7 +848,7 @@ struct BookRunner {
         // chunk size from the slice alone: at most kChunkNormals normals per lane, split into
         // at least kMinChunksPerRep chunks per replica where the slice has that many groups (a
         // round whose few slices are small still spreads over the GPU), at most kMaxChunksPerRep
-        const long long D = (long long)opts[i].n_assets * nfine(l);
+        const long long D = (long long)book_width(opts[i]) * nfine(l);
         const uint64_t G = ((uint64_t)x.offset + x.n_points - 1) / 32 + 1 - (x.offset >> 5);
         uint64_t gpc = std::min<uint64_t>((uint64_t)std::max<long long>(1, kChunkNormals / D),
                                           std::max<uint64_t>(1, G / kMinChunksPerRep));
@@ -725,6 +865,11 @@ struct BookRunner {
         // by basket width: a class kernel's warps then take chunks of one width at a time, so one
         // specialisation's code is hot in the instruction cache instead of four
         std::stable_sort(sp.begin(), sp.end(), [&](const BookSpec& a, const BookSpec& b) {
+            const int ca = book_class_of(opts[a.opt]), cb = book_class_of(opts[b.opt]);
+            if (ca != cb) return ca < cb;
+            if (ca == kSingleClass)   // one model / payoff's code at a time
+                return opts[a.opt].model->kind * 16 + opts[a.opt].payoff->kind <
+                       opts[b.opt].model->kind * 16 + opts[b.opt].payoff->kind;
             return opts[a.opt].n_assets < opts[b.opt].n_assets;
         });
         int* h = (int*)s.hspecs.ensure(sizeof(int) * kHdrInts + sizeof(BookSpec) * std::max<size_t>(max_specs, 1));
@@ -733,9 +878,9 @@ struct BookRunner {
         int chunk = 0;
         size_t k = 0;
         for (int c = 0; c < kBookClasses; c++) {
-            h[2 + c] = chunk;
-            h[7 + c] = (int)k;
-            for (; k < sp.size() && book_class(opts[sp[k].opt].n_assets) == c; k++) {
+            h[kHdrChunk0 + c] = chunk;
+            h[kHdrSlice0 + c] = (int)k;
+            for (; k < sp.size() && book_class_of(opts[sp[k].opt]) == c; k++) {
                 sp[k].chunk0 = chunk;
                 MCQ_REQUIRE((long long)chunk + (long long)R * sp[k].cpr < INT_MAX, MCQ_ERR_RANGE, "book: chunk count overflow");
                 chunk += R * sp[k].cpr;
@@ -743,8 +888,8 @@ struct BookRunner {
             }
         }
         h[0] = (int)sp.size();
-        h[1] = h[2 + kBookClasses] = chunk;
-        h[7 + kBookClasses] = (int)sp.size();
+        h[1] = h[kHdrChunk0 + kBookClasses] = chunk;
+        h[kHdrSlice0 + kBookClasses] = (int)sp.size();
         s.specs.ensure(sizeof(BookSpec) * std::max<size_t>(max_specs, 1));
         s.hdr.ensure(sizeof(int) * kHdrInts);
         s.out.ensure(sizeof(double) * kBookOut * std::max<size_t>(max_specs, 1));
@@ -755,7 +900,7 @@ struct BookRunner {
     }
 
     static int grid_of(int cls, int variant) {
-        static int per_sm[kBookClasses][kBookVariants] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
+        static int per_sm[kBookClasses][kBookVariants] = {{-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}, {-1, -1}};
         if (per_sm[cls][variant] < 0) {
             const void* fn = (const void*)book_fn(cls, variant);
             MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)book_smem(cls)));
@@ -871,7 +1016,7 @@ struct BookRunner {
         for (int l = 0; l <= max_L_all; l++) slots.emplace_back(E.ws(1 + l));
         std::vector<BookSpec> one(1);
         for (int i = 0; i < n; i++) {
-            const int cls = book_class(opts[i].n_assets);
+            const int cls = book_class_of(opts[i]);
             for (;;) {
                 plan(i);
                 OptState& s = st[i];
@@ -887,7 +1032,7 @@ struct BookRunner {
                     const int chunks = upload(sl, one);
                     const BookArgs a = args(sl);
                     launch_book_tuned(cls, a, chunks,
-                                      (double)R * (double)one[0].n_points * (double)opts[i].n_assets * (double)nfine(l),
+                                      (double)R * (double)one[0].n_points * (double)book_width(opts[i]) * (double)nfine(l),
                                       sl.stream);
                     launch_fin(a, 1, sl.stream);
                     double* ho = (double*)sl.hout.ensure(sizeof(double) * kBookOut);
@@ -917,7 +1062,8 @@ struct BookRunner {
                 r.price += s.E[l];
                 if (s.N[l]) vs += s.sig2[l] / ((double)s.N[l] * (double)R);
                 Nt += s.N[l] * R;
-                for (int a = 0; a < opts[i].n_assets; a++) r.delta[a] += s.Dl[l][a];
+                if (!opts[i].model)
+                    for (int a = 0; a < opts[i].n_assets; a++) r.delta[a] += s.Dl[l][a];
             }
             r.std_error = std::sqrt(vs);
             r.n_samples = Nt;
@@ -942,8 +1088,8 @@ void book_level_sums(const mcq_book_option& opt, const mcq_mlmc_cfg& ml, const m
     std::vector<BookSpec> one(1, b.make_spec(0, level, n_points));
     grow(s.records, sizeof(double) * kBookNST * (size_t)b.R * one[0].cpr);
     const int chunks = b.upload(s, one);
-    const int cls = book_class(opt.n_assets);
-    b.launch_book_tuned(cls, b.args(s), chunks, (double)b.R * (double)n_points * (double)opt.n_assets * (double)b.nfine(level),
+    const int cls = book_class_of(opt);
+    b.launch_book_tuned(cls, b.args(s), chunks, (double)b.R * (double)n_points * (double)book_width(opt) * (double)b.nfine(level),
                         s.stream);
     std::vector<double> rec((size_t)chunks * kBookNST);
     MCQ_CUDA(cudaMemcpyAsync(rec.data(), s.records.p, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost, s.stream));

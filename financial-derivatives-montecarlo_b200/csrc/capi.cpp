@@ -521,6 +521,8 @@ struct mcq_book_s {
     struct Owned {
         mcq_book_option o;
         std::vector<double> S0, sigma, weights, L;
+        mcq_model model{};       // a single-asset option's model and payoff (no arrays: GBM,
+        mcq_payoff payoff{};     // Heston, parametric Dupire)
     };
     std::vector<Owned> items;
 };
@@ -539,19 +541,31 @@ int mcq_book_submit(mcq_book b, const mcq_book_option* opts, int n) {
     std::vector<mcq_book_s::Owned> add((size_t)n);
     for (int i = 0; i < n; i++) {
         const mcq_book_option& o = opts[i];
+        mcq_book_s::Owned& w = add[(size_t)i];
+        w.o = o;
+        if (o.model) {   // single-asset option: copy its model and payoff
+            MCQ_REQUIRE(o.payoff, MCQ_ERR_INVALID, "book option " + std::to_string(i) + ": a model needs a payoff");
+            w.model = *o.model;
+            w.payoff = *o.payoff;
+            w.o.S0 = w.o.sigma = w.o.weights = w.o.L = nullptr;
+            continue;
+        }
         MCQ_REQUIRE(o.n_assets >= 1 && o.n_assets <= MCQ_BOOK_MAX_ASSETS, MCQ_ERR_UNSUPPORTED,
                     "book option " + std::to_string(i) + ": needs 1..16 assets");
         MCQ_REQUIRE(o.S0 && o.sigma, MCQ_ERR_INVALID, "book option " + std::to_string(i) + ": needs S0 and sigma");
         const int d = o.n_assets;
-        mcq_book_s::Owned& w = add[(size_t)i];
-        w.o = o;
         w.S0.assign(o.S0, o.S0 + d);
         w.sigma.assign(o.sigma, o.sigma + d);
         if (o.weights) w.weights.assign(o.weights, o.weights + d);
         if (o.L) w.L.assign(o.L, o.L + (size_t)d * d);
     }
     for (auto& w : add) b->items.push_back(std::move(w));
-    for (auto& w : b->items) {   // re-point at the owned arrays (push_back may have moved them)
+    for (auto& w : b->items) {   // re-point at the owned copies (push_back may have moved them)
+        if (w.o.model) {
+            w.o.model = &w.model;
+            w.o.payoff = &w.payoff;
+            continue;
+        }
         w.o.S0 = w.S0.data();
         w.o.sigma = w.sigma.data();
         w.o.weights = w.weights.empty() ? nullptr : w.weights.data();

@@ -76,7 +76,7 @@ BOOK_BATCHED, BOOK_PLAIN = 0, 1
 class BookOption(C.Structure):
     _fields_ = [("n_assets", C.c_int32), ("max_L", C.c_int32), ("K", C.c_double), ("r", C.c_double),
                 ("T", C.c_double), ("eps", C.c_double), ("S0", _pd), ("sigma", _pd), ("weights", _pd),
-                ("L", _pd)]
+                ("L", _pd), ("model", C.POINTER(Model)), ("payoff", C.POINTER(Payoff))]
 
 
 class BookResult(C.Structure):
@@ -191,6 +191,39 @@ def book_option(S0, sigma, K, r, T, eps, max_L, weights=None, L=None):
         o.L = pl
         keep.append(l)
     return _keep(o, *keep)
+
+
+def book_single(model, payoff, eps, max_L):
+    """A single-asset option of a book: `model` (GBM, Heston, parametric Dupire) with `payoff`,
+    priced by MLQMC to eps with levels up to max_L (no deltas)."""
+    o = BookOption()
+    o.n_assets, o.max_L, o.eps, o.T = 1, int(max_L), eps, model.T
+    o.model, o.payoff = C.pointer(model), C.pointer(payoff)
+    return _keep(o, model, payoff)
+
+
+def mixed_singles(n=256, seed=6, r=0.02):
+    """Single-asset options for a mixed book: models GBM (sigma ~ U[0.1, 0.4]), Heston (the
+    benchmark's Heston parameters with xi ~ U[0.2, 0.5], rho ~ U[-0.8, -0.3]) and parametric Dupire
+    (sigma0 ~ U[0.15, 0.3]) in turn, S0 100, T ~ U[0.25, 2], with European, Asian, lookback and
+    down-and-out (B = 80) payoffs in turn, K = 100 U[0.9, 1.1], eps ~ U[5e-4, 5e-3] and max_L 6
+    (M = 2, n0 = 1: 64 finest steps)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        T = float(rng.uniform(0.25, 2.0))
+        kind = i % 3
+        if kind == 0:
+            m = gbm(100.0, r, float(rng.uniform(0.1, 0.4)), T)
+        elif kind == 1:
+            m = heston(100.0, r, 2.0, 0.04, float(rng.uniform(0.2, 0.5)), float(rng.uniform(-0.8, -0.3)), 0.04, T)
+        else:
+            m = dupire(100.0, r, float(rng.uniform(0.15, 0.3)), 0.5, 0.7, T)
+        K = float(100.0 * rng.uniform(0.9, 1.1))
+        pk = (i // 3) % 4
+        p = (european(K, r, T), asian(K), lookback(0.2), barrier_down_out(K, 80.0, 0.2, r, T))[pk]
+        out.append(book_single(m, p, float(rng.uniform(5e-4, 5e-3)), 6))
+    return out
 
 
 def config5_book(n=4096, seed=5, r=0.03):

@@ -164,9 +164,13 @@ typedef struct mcq_greeks {
     double  path_steps;                           /* forward + recompute + reverse path-steps */
 } mcq_greeks;
 
-/* One option of a batched book (mcq_book_price): a call on a weighted basket of correlated
-   GBM assets, max(sum_a w_a S_a(T) - K, 0) e^{-rT}, drift r, priced by MLQMC to its own eps
-   with the pathwise delta per asset.  No counterpart in the reference. */
+/* One option of a batched book (mcq_book_price), priced by MLQMC to its own eps.  Either
+   (model == NULL) a call on a weighted basket of correlated GBM assets,
+   max(sum_a w_a S_a(T) - K, 0) e^{-rT}, drift r, with the pathwise delta per asset; or
+   (model != NULL) a single-asset option: `model` (GBM, Heston or parametric Dupire; its T is the
+   maturity) with `payoff` (European, Asian, geometric Asian, lookback, up- or down-and-out
+   barrier), the coupled level pair of mcq_run_mlqmc; then n_assets, K, r, T, S0, sigma, weights
+   and L are not read and no deltas are returned.  No counterpart in the reference. */
 #define MCQ_BOOK_MAX_ASSETS 16
 typedef struct mcq_book_option {
     int32_t n_assets;             /* 1..16 */
@@ -176,6 +180,8 @@ typedef struct mcq_book_option {
     const double* sigma;          /* [n_assets] */
     const double* weights;        /* [n_assets]; NULL: equal weights */
     const double* L;              /* [n_assets^2] row-major lower Cholesky; NULL: uncorrelated */
+    const mcq_model* model;       /* NULL: the basket above; else a single-asset model */
+    const mcq_payoff* payoff;     /* the single-asset option's payoff (with model) */
 } mcq_book_option;
 
 typedef struct mcq_book_result {

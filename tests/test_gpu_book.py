@@ -123,19 +123,20 @@ def test_book_delta_matches_bump_and_revalue(gpu):
 
 def test_book_config5_sample_prices_converge(gpu):
     """A sample of the synthetic book: every option either passes the bias test or has grown
-    to its finest level, its SE meets its own eps, and the one-asset options agree with
-    Black–Scholes."""
+    to its finest level, every option's SE meets its own eps (converged or not), and the one-asset
+    options that converged agree with Black–Scholes within the stopping test's bias bound
+    eps / sqrt(2) plus 3 standard errors."""
     book = gpu.config5_book(n=64, seed=5)
     for o in book:
         o.eps = 4 * o.eps                        # keep the test short: coarser targets
     res, st = gpu.book_price(book, gpu.BOOK_BATCHED)
-    assert st["rounds"] >= 2 and st["launches"] == 5 * st["rounds"]   # 4 width classes + finalize
+    assert st["rounds"] >= 2 and st["launches"] == 6 * st["rounds"]   # 5 class kernels + finalize
     for o, r in zip(book, res):
         assert np.isfinite(r["price"]) and r["price"] >= 0
-        assert r["std_error"] <= o.eps * 1.01 or not r["converged"], (o.eps, r)
+        assert r["std_error"] <= o.eps * 1.01, (o.eps, r)
         if o.n_assets == 1 and r["converged"]:
             S, s = o.S0[0], o.sigma[0]
-            assert abs(r["price"] - orc_bs(S, o.K, o.T, o.r, s)) < 3 * r["std_error"] + 10 * o.eps
+            assert abs(r["price"] - orc_bs(S, o.K, o.T, o.r, s)) < 3 * r["std_error"] + o.eps / math.sqrt(2)
         assert r["converged"] or r["levels"] == o.max_L + 1, (o.max_L, r)
 
 
@@ -267,3 +268,70 @@ def test_book_class_variants_are_bit_identical(gpu):
         for a, b in zip(res[0], r):
             assert a["price"] == b["price"] and a["n_samples"] == b["n_samples"]
             assert np.array_equal(a["delta"], b["delta"])
+
+
+def _single(gpu, model, pay, eps=5e-3, max_L=6):
+    m = {"gbm": lambda: gpu.gbm(100.0, 0.02, 0.25, 1.0),
+         "heston": lambda: gpu.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0),
+         "dupire": lambda: gpu.dupire(100.0, 0.02, 0.2, 0.5, 0.7, 1.0)}[model]()
+    p = {"eur": lambda: gpu.european(100.0, 0.02, 1.0), "asian": lambda: gpu.asian(100.0),
+         "lookback": lambda: gpu.lookback(0.2), "downout": lambda: gpu.barrier_down_out(100.0, 85.0, 0.2, 0.02, 1.0),
+         "upout": lambda: gpu.barrier_up_out(100.0, 130.0, 0.2, 0.02, 1.0), "geom": lambda: gpu.geom_asian(100.0)}[pay]()
+    return gpu.book_single(m, p, eps, max_L), m, p
+
+
+@pytest.mark.parametrize("model,pay,level", [("gbm", "eur", 0), ("gbm", "asian", 3), ("heston", "lookback", 2),
+                                             ("heston", "downout", 4), ("dupire", "eur", 1), ("dupire", "upout", 5),
+                                             ("gbm", "geom", 2)])
+def test_book_single_asset_slice_sums_match_oracle(gpu, orc, model, pay, level):
+    """A single-asset book option's slice through the book's single-asset class kernel (the fused
+    pass's coupled consumer) against the FP64 oracle's coupled level pair on the same points
+    (salts salt_base + level R + r, a ragged offset and count)."""
+    o, m, p = _single(gpu, model, pay)
+    ml, qc = gpu.mlmc_cfg(M=2, n0_steps=1), gpu.qmc_cfg(R=4, salt_base=42)
+    offset, N = 37, 1000
+    g = gpu.book_level_sums(o, level, offset, N, ml, qc)
+    ref = orc.level_sums(m, p, 2 ** level, 2 if level else 0, None, use_sobol=True, salt_base=42 + level * 4, R=4,
+                         offset=offset, N=N)
+    extra = 60.0 if pay in ("downout", "upout") else 0.0
+    for q in (0, 2):
+        scale = N + abs(ref[:, 2]).max()
+        assert np.abs(g[:, q] - ref[:, q]).max() < 2e-5 * scale + extra, (q, g[:, q], ref[:, q])
+
+
+@pytest.mark.parametrize("model,pay", [("gbm", "eur"), ("heston", "lookback"), ("dupire", "asian")])
+def test_book_single_asset_agrees_with_run_mlqmc(gpu, model, pay):
+    """A single-asset option priced in the book and by mcq_run_mlqmc: the same model, payoff, levels,
+    salts and point counts, so the same paths; the level sums are reduced in different orders, so
+    the prices agree to the rounding of the sums unless a rounding tips a sample count, and always
+    within 3 standard errors of the difference."""
+    o, m, p = _single(gpu, model, pay, eps=3e-3, max_L=6)
+    ml, qc = gpu.mlmc_cfg(M=2, n0_steps=1, max_L=6), gpu.qmc_cfg(R=16)
+    rb, _ = gpu.book_price([o], gpu.BOOK_BATCHED, ml, qc)
+    q = gpu.run_mlqmc(m, p, 3e-3, ml, qc)
+    assert abs(rb[0]["price"] - q["price"]) < 3 * np.hypot(rb[0]["std_error"], q["std_error"]), (rb[0], q)
+    assert rb[0]["levels"] == q["levels"]
+    assert not rb[0]["delta"].any()
+
+
+def test_mixed_book_batched_equals_plain_and_black_scholes(gpu):
+    """Baskets and single-asset options in one book: batched equals plain bit for bit, and the GBM
+    European singles that converged lie within the stopping test's bias bound plus 3 standard errors
+    of Black-Scholes."""
+    book = gpu.config5_book(n=8, seed=77) + gpu.mixed_singles(n=12, seed=3)
+    for o in book:
+        o.eps = 5 * o.eps
+    rb, _ = gpu.book_price(book, gpu.BOOK_BATCHED)
+    rp, _ = gpu.book_price(book, gpu.BOOK_PLAIN)
+    for a, b in zip(rb, rp):
+        assert a["price"] == b["price"] and a["n_samples"] == b["n_samples"]
+        assert np.array_equal(a["delta"], b["delta"])
+    checked = 0
+    for o, r in zip(book, rb):
+        if o.model and o.model.contents.kind == gpu.GBM and o.payoff.contents.kind == gpu.EUROPEAN and r["converged"]:
+            m, p = o.model.contents, o.payoff.contents
+            d1 = (math.log(m.S0 / p.K) + (m.mu + 0.5 * m.sigma ** 2) * m.T) / (m.sigma * math.sqrt(m.T))
+            bs = m.S0 * _ncdf(d1) - p.K * math.exp(-p.r * p.T) * _ncdf(d1 - m.sigma * math.sqrt(m.T))
+            assert abs(r["price"] - bs) < o.eps / math.sqrt(2) + 3 * r["std_error"], (r, bs)
+            checked += 1
+    assert checked >= 1
