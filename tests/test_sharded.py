@@ -89,3 +89,43 @@ def test_replica_blocks_cover_every_replica_once(eng):
     with pytest.raises(ValueError):
         sh.replica_block(4, 2, 2)
     assert sh.book_share(7, 3, 1) == [1, 4]
+
+
+def _oracle_level(l, r0, nr, offset, n, R=5, salt_base=42, M=2):
+    import oracle_py as orc
+    T = orc.T
+    m, p = T.gbm(100.0, 0.05, 0.2, 1.0), T.european(100.0, 0.05, 1.0)
+    return orc.level_sums(m, p, M ** l, M if l else 0, None, use_sobol=True, salt_base=salt_base + l * R + r0,
+                          R=nr, offset=offset, N=n, threads=1)
+
+
+def _rank_mlqmc(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from conftest import load_engine
+    load_engine()
+    import fdmc_b200.sharded as sh
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        r = sh.run_mlqmc_sharded(_oracle_level, 5, 2e-2, M=2, max_L=6, pilot_n=200)
+        np.save(os.path.join(out_dir, "mlqmc_%d.npy" % rank),
+                np.array([r["price"], r["std_error"], r["n_samples"], r["levels"], float(r["converged"])]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_mlqmc_equals_one_process(eng, tmp_path):
+    """The sharded MLQMC loop (each level's 5 replicas split 3 + 2 over two gloo ranks, one
+    all-reduce per collect) gives the one-process result bit for bit when each replica's level sums
+    do not depend on its launch's other replicas (the oracle's), and prices the GBM European close
+    to Black-Scholes."""
+    import fdmc_b200.sharded as sh
+    one = sh.run_mlqmc_sharded(_oracle_level, 5, 2e-2, M=2, max_L=6, pilot_n=200)
+    assert one["levels"] >= 3
+    mp.spawn(_rank_mlqmc, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    for rank in range(2):
+        got = np.load(tmp_path / ("mlqmc_%d.npy" % rank))
+        assert got[0] == one["price"] and got[1] == one["std_error"], (got, one)
+        assert got[2] == one["n_samples"] and got[3] == one["levels"]
+    import oracle_py as orc
+    assert abs(one["price"] - orc.bs_call(100, 100, 1, 0.05, 0.2)) < 3 * one["std_error"] + 2e-2 / np.sqrt(2)
