@@ -304,8 +304,10 @@ def book_bench(eng, n, n_loose, orv):
                        "launches": st["launches"], "normals_per_s": normals / tmax,
                        "path_steps_per_s": psteps / tmax}
         d["batched_over_plain"] = d["batched"]["options_per_s"] / d["plain"]["options_per_s"]
-        d["bit_identical"] = all(a["price"] == b["price"] and bool((a["delta"] == b["delta"]).all())
+        same = lambda x, y: x == y or (x != x and y != y)   # noqa: E731  (NaN in both modes counts as equal)
+        d["bit_identical"] = all(same(a["price"], b["price"]) and bool((a["delta"] == b["delta"]).all())
                                  for a, b in zip(res["batched"], res["plain"]))
+        d["non_finite"] = sum(1 for a in res["batched"] if not math.isfinite(a["price"]))
         d["checks"] = book_checks(eng, opts, res["batched"], orv) if world == 1 else None
         d["converged"] = sum(1 for x in res["batched"] if x["converged"])
         return d

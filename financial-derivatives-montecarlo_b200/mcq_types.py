@@ -206,8 +206,11 @@ def mixed_singles(n=256, seed=6, r=0.02):
     """Single-asset options for a mixed book: models GBM (sigma ~ U[0.1, 0.4]), Heston (the
     benchmark's Heston parameters with xi ~ U[0.2, 0.5], rho ~ U[-0.8, -0.3]) and parametric Dupire
     (sigma0 ~ U[0.15, 0.3]) in turn, S0 100, T ~ U[0.25, 2], with European, Asian, lookback and
-    down-and-out (B = 80) payoffs in turn, K = 100 U[0.9, 1.1], eps ~ U[5e-4, 5e-3] and max_L 6
-    (M = 2, n0 = 1: 64 finest steps)."""
+    down-and-out (B = 80) payoffs in turn (Dupire options take the down-and-out call in place of the
+    lookback: on the coarsest levels an Euler step spans up to T, a path can step below 0, and the
+    local volatility (S / S0)^(beta - 1) is then NaN, which the lookback's S_T - min S carries into
+    the price as the reference's formulas do), K = 100 U[0.9, 1.1], eps ~ U[5e-4, 5e-3] and
+    max_L 6 (M = 2, n0 = 1: 64 finest steps)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
@@ -221,6 +224,8 @@ def mixed_singles(n=256, seed=6, r=0.02):
             m = dupire(100.0, r, float(rng.uniform(0.15, 0.3)), 0.5, 0.7, T)
         K = float(100.0 * rng.uniform(0.9, 1.1))
         pk = (i // 3) % 4
+        if kind == 2 and pk == 2:
+            pk = 3
         p = (european(K, r, T), asian(K), lookback(0.2), barrier_down_out(K, 80.0, 0.2, r, T))[pk]
         out.append(book_single(m, p, float(rng.uniform(5e-4, 5e-3)), 6))
     return out

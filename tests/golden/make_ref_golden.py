@@ -19,6 +19,9 @@ python tests/golden/make_ref_golden.py --levels writes ref_golden_levels.npz (+ 
     scrambled Sobol normals (golden_cases.is_cases).
 A case whose window holds a point with u = 1 (scrambled word >= 0xFFFFFF80) moves to the next
 salt (+ 1000) until it has none; the JSON records the salt used.
+
+python tests/golden/make_ref_golden.py --timing [N] prints the device time of the reference's own
+pass for the RQMC Asian workload at 32 replicas x N points (default 2^20), raw and bridge.
 """
 import ctypes as C
 import json
@@ -168,8 +171,24 @@ def main_levels(out):
         json.dump(meta, f, indent=1)
 
 
+def main_timing(n_per_replica):
+    """Device time of the reference's own generate -> transform -> price steps for the RQMC Asian
+    workload (GBM, 256 steps, 32 replicas x n_per_replica points), raw and Brownian-bridge
+    ordering, after one warm-up pass each: the GPU path the engine's fused pass replaces."""
+    m, p = T.gbm(100.0, 0.03, 0.25, 1.0), T.asian(100.0)
+    out = {}
+    for name, mode in (("raw", T.RAW), ("bridge", T.BB)):
+        ref_pass(m, p, 256, mode, 42, 1, 0, 1 << 14)
+        sums, ms = ref_pass(m, p, 256, mode, 42, 32, 0, n_per_replica)
+        out[name] = {"ms": ms, "path_steps_per_s": 32 * n_per_replica * 256 / (ms * 1e-3),
+                     "price": float((sums[:, 0] / n_per_replica).mean())}
+    print(json.dumps({"reference_gpu_asian_256_R32": dict(out, points_per_replica=n_per_replica)}))
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "--levels":
+    if len(sys.argv) > 1 and sys.argv[1] == "--timing":
+        main_timing(int(sys.argv[2]) if len(sys.argv) > 2 else 1 << 20)
+    elif len(sys.argv) > 1 and sys.argv[1] == "--levels":
         main_levels(os.path.join(HERE, "ref_golden_levels.npz"))
     else:
         main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "ref_golden.npz"))
