@@ -15,6 +15,8 @@ runs on the GPU).  What each value is:
                          down-and-out call (K 100, B 80): the FP64 oracle's MLQMC driver
                          (oracle_py.run_mlqmc, the arithmetic of run_mlqmc_cuda) at eps = 5e-4,
                          M = 4, 4 steps on level 0, L <= 8, R = 16, salts 1042...
+  asian_gbm_256_engine_points  the same contract's FP64 per-replica sums on the benchmark pass's own
+                         points (salts 42.., 32 x 2^20), for a same-points check of the full-size pass.
   adjoint_localvol_asian the adjoint workload (64 x 32 local-vol grid, Asian call, T = 2, 512
                          steps): price from FP64 oracle RQMC over 16 x 2^20 independent points
                          (salts 1042..); delta, rho and vega (parallel shift of the grid) as FP64
@@ -75,6 +77,16 @@ def asian_gbm_256():
     return {"value": float(rm.mean()), "se": float(rm.std(ddof=1) / np.sqrt(R)),
             "kind": f"FP64 oracle RQMC, {R} replicas x 2^22 points, 256 Euler steps, salts {SALT}..",
             "geom_closed_form": orc.geom_asian(100.0, 100.0, 1.0, 0.03, 0.25, 256)}
+
+
+def asian_engine_points():
+    """FP64 per-replica sums on the benchmark pass's own points (salts 42.., 2^20 points per replica):
+    the engine's full-size pass is checked against them replica by replica."""
+    m, p = T.gbm(100.0, 0.03, 0.25, 1.0), T.asian(100.0)
+    R, N = 32, 1 << 20
+    s = orc.qmc_sums(m, p, 256, None, 42, R, 0, N)
+    return {"sums": s.tolist(), "R": R, "N": N, "salt_base": 42,
+            "kind": "FP64 oracle per-replica {sum Y, sum Y^2}, the bench pass's points (salts 42.., 2^20 per replica)"}
 
 
 def heston(pay):
@@ -140,6 +152,7 @@ def main():
     ap.add_argument("--book-sample", type=int, default=4)
     a = ap.parse_args()
     jobs = [("mc_gbm_european", mc_gbm_european), ("asian_gbm_256", asian_gbm_256),
+            ("asian_gbm_256_engine_points", asian_engine_points),
             ("adjoint_localvol_asian", adjoint_localvol),
             ("mlqmc_heston_lookback", lambda: heston("lookback")),
             ("mlqmc_heston_down_out", lambda: heston("down_out")),

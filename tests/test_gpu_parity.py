@@ -363,3 +363,20 @@ def test_heston_fine_levels_vs_oracle(gpu, orc, pay, level, R, N):
         extra = 60.0 / N if pay == "downout" else 0.0
         assert abs(g[r, 2] / N - o[r, 2] / N) < 2e-4 * sc + extra, (level, r, g[r], o[r])
         assert abs(g[r, 0] / N - o[r, 0] / N) < 2e-4 * sc + extra, (level, r, g[r], o[r])
+
+
+def test_bench_pass_at_full_size_vs_fp64_oracle(gpu):
+    """The benchmark's own pass (arithmetic Asian, 256 steps, 32 replicas x 2^20 scrambled-Sobol
+    points) against the FP64 oracle's per-replica sums on the same points, replica by replica
+    (tests/golden/oracle_values.json, written by make_oracle_values.py): FP32 paths, FP64 sums."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "oracle_values.json")) as f:
+        ref = json.load(f)["asian_gbm_256_engine_points"]
+    R, N = ref["R"], ref["N"]
+    o = np.array(ref["sums"])
+    g = gpu.qmc_pass(gpu.gbm(100.0, 0.03, 0.25, 1.0), gpu.asian(100.0), 256, salt_base=ref["salt_base"], R=R,
+                     offset=0, n_points=N)
+    gm, om = g[:, 0] / N, o[:, 0] / N
+    assert np.abs(gm - om).max() < 2e-5 * (1 + np.abs(om).max()), np.abs(gm - om).max()
+    assert abs(gm.mean() - om.mean()) < 5e-6 * om.mean()
