@@ -13,8 +13,13 @@ scrambled Sobol dimensions, R = 32 replicas with salts 42.., raw noise ordering.
          eps = 1e-3 from 2^14 points per replica, doubling until var_of_means < eps^2/2, with
          host structs in and the result read back; path-steps of the whole adaptive run over
          host wall time.
-Multi-GPU (torchrun): every rank prices its own 32 replicas (salts offset by rank), no
-collective on the data path; max over ranks of the device time; "scaling": "weak".
+Multi-GPU (torchrun): one estimator of 32 N replicas split in blocks of 32 over the N ranks
+(rank k owns the replicas of salts 42 + 32 k ..), the only exchange the estimator has: after each
+pass one all-reduce of the [32 N][2] FP64 per-replica sums (every slot with one contributor, so
+the reduced sums are the one-process sums bit for bit) gives every rank the estimator; max over
+ranks of the device time; "scaling": "weak".  The e2e leg at N > 1 runs the same split through
+the adaptive doubling loop (sharded.run_qmc_sharded over mcq_qmc_pass, one all-reduce per
+doubling) with R = 32 N.
 --impl reference times the reference algorithm's CPU restatement (the oracle) on the host
 cores on a bounded sample of the same workload (the reference has no CPU path of its own).
 """
@@ -467,8 +472,14 @@ def main():
     sp = stream.cuda_stream
     assert sp != 0
 
+    gsums = torch.zeros(world * REPS * 2, dtype=torch.float64, device="cuda") if world > 1 else sums
+
     def one_pass():
         eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, salt_base=salt, R=REPS, offset=0, n_points=N)
+        if world > 1:   # the estimator over all ranks' replicas, on every rank (NCCL on `stream`)
+            gsums.zero_()
+            gsums[rank * REPS * 2:(rank + 1) * REPS * 2].copy_(sums)
+            torch.distributed.all_reduce(gsums, op=torch.distributed.ReduceOp.SUM)
 
     # the clock sampler starts before the warm-up (nvidia-smi needs a moment to start) and its
     # summary keeps the samples from the start of the timed region on
@@ -503,10 +514,10 @@ def main():
         total_ms = float(t.item())
     ps_per_step = REPS * N * STEPS
     value = world * ps_per_step * args.steps / (total_ms * 1e-3)
-    chk = sums.cpu().numpy().reshape(REPS, 2)
+    chk = gsums.cpu().numpy().reshape(world * REPS, 2)
     rmeans = chk[:, 0] / N
     price = float(rmeans.mean())
-    price_se = float(rmeans.std(ddof=1) / math.sqrt(REPS))
+    price_se = float(rmeans.std(ddof=1) / math.sqrt(world * REPS))
 
     # the same workload under Brownian-bridge and PCA (tcgen05) ordering, same timing rules
     variants = {}
@@ -540,23 +551,40 @@ def main():
     gm = sums.cpu().numpy().reshape(REPS, 2)[:, 0] / N
     geom_check = {"price": float(gm.mean()), "std_error": float(gm.std(ddof=1) / math.sqrt(REPS))}
 
-    # e2e: the reference-facing adaptive driver with host structs
+    # e2e: the reference-facing adaptive driver with host structs (one rank), or the same doubling
+    # loop with the replicas split over the ranks (host buffers through mcq_qmc_pass per block)
     cfg = eng.qmc_cfg(R=REPS, N0_per_replica=1 << 14, salt_base=salt)
-    eng.run_qmc(m, p, 1e-3, STEPS, cfg)   # warm-up (tables, streams)
+    if world == 1:
+        def e2e_run():
+            r = eng.run_qmc(m, p, 1e-3, STEPS, cfg)
+            return r, r["path_steps"]
+    else:
+        import importlib
+        sharded = importlib.import_module("fdmc_b200.sharded")
+
+        def e2e_run():
+            def pass_fn(r0, nr, offset, n):
+                return eng.qmc_pass(m, p, STEPS, salt_base=SALT + r0, R=nr, offset=offset, n_points=n)
+            r = sharded.run_qmc_sharded(pass_fn, world * REPS, 1e-3, 1 << 14, max_doublings=cfg.max_doublings,
+                                        device="cuda")
+            lo, hi = sharded.replica_block(world * REPS, world, rank)
+            return r, float(r["n_samples"]) / (world * REPS) * (hi - lo) * STEPS
+    e2e_run()   # warm-up (tables, streams)
     e2e_ps, e2e_t, e2e_last = 0.0, 0.0, None
     for _ in range(args.e2e_runs):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = eng.run_qmc(m, p, 1e-3, STEPS, cfg)
+        r, ps = e2e_run()
         e2e_t += time.perf_counter() - t0
-        e2e_ps += r["path_steps"]
+        e2e_ps += ps
         e2e_last = r
     if world > 1:
-        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_t = float(t.item())
-    e2e_value = world * e2e_ps / e2e_t
-    doublings = max(1, int(round(__import__("math").log2(e2e_last["n_samples"] / (REPS << 14)))) + 1)
+        t = torch.tensor([e2e_t, e2e_ps], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
+        e2e_t, e2e_ps = float(t[0].item()), float(t[1].item())
+    e2e_value = e2e_ps / e2e_t
+    doublings = max(1, int(round(math.log2(e2e_last["n_samples"] / (world * REPS << 14)))) + 1)
     import ctypes
     h2d_e2e = ctypes.sizeof(m) + ctypes.sizeof(p) + ctypes.sizeof(cfg)
 

@@ -27,8 +27,8 @@ EXPORTS = [
     "mcq_run_mc", "mcq_run_mc_fixed", "mcq_run_qmc", "mcq_run_mlmc", "mcq_run_mlqmc", "mcq_cv_pilot",
     "mcq_run_mc_cv", "mcq_run_qmc_cv", "mcq_run_is", "mcq_qmc_pass", "mcq_qmc_pass_device",
     "mcq_mc_pass", "mcq_level_pass", "mcq_is_pass", "mcq_sobol_hh_u32", "mcq_sobol_hh_normal", "mcq_philox4x32_10",
-    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_debug_wait_timeout", "mcq_qmc_pass_noalloc",
-    "mcq_adjoint",
+    "mcq_bb_tables", "mcq_pca_matrix", "mcq_debug_pass_dump", "mcq_debug_wait_timeout",
+    "mcq_debug_last_pass_layout", "mcq_qmc_pass_noalloc", "mcq_adjoint",
     "mcq_book_price", "mcq_book_level_sums", "mcq_book_create", "mcq_book_submit", "mcq_book_size",
     "mcq_book_run", "mcq_book_clear", "mcq_book_free",
 ]
@@ -367,6 +367,13 @@ def debug_pass_dump(m, n_steps, noise=RAW, bb=None, use_sobol=True, seed=0, salt
                                      C.c_uint32(seed), C.c_uint32(salt_base), C.c_int(R), C.c_uint32(offset),
                                      C.c_int64(n_points), C.c_int(flags), out.ctypes.data_as(_P(C.c_float))))
     return out
+
+
+def debug_last_pass_layout():
+    """(groups per work item, carried Sobol start words per warp) of the last fused pass."""
+    g, c = C.c_int(0), C.c_int(0)
+    _check(lib().mcq_debug_last_pass_layout(C.byref(g), C.byref(c)))
+    return g.value, c.value
 
 
 def sobol_hh_u32(salt, dim0, nd, offset, n):

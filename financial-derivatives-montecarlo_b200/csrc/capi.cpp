@@ -672,6 +672,15 @@ int mcq_debug_wait_timeout(uint32_t polls) {
     API_END
 }
 
+int mcq_debug_last_pass_layout(int* groups_per_item, int* carry_words) {
+    API_BEGIN
+    MCQ_REQUIRE(groups_per_item && carry_words, MCQ_ERR_INVALID, "NULL argument");
+    Engine& E = engine();
+    *groups_per_item = E.last_gpi;
+    *carry_words = E.last_carry;
+    API_END
+}
+
 int mcq_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     if (!ctr || !key || !out) { g_last_error = "NULL argument"; return MCQ_ERR_INVALID; }
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];

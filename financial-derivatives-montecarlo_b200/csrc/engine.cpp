@@ -96,6 +96,7 @@ void ensure_ready(int device) {
                     " is sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
     E.device = dev;
     E.sm_count = prop.multiProcessorCount;
+    E.smem_optin = (int)prop.sharedMemPerBlockOptin;
     // JoeKuo6 direction vectors, as ensure_sobol_dirvectors_uploaded (methods_cuda.cu:764-775).
     curandDirectionVectors32_t* hv = nullptr;
     MCQ_REQUIRE(curandGetDirectionVectors32(&hv, CURAND_DIRECTION_VECTORS_32_JOEKUO6) ==
@@ -312,17 +313,25 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
 // ------------------------------------------------------------------ launcher
 
 
+// Resident blocks per SM of kernel `fn` at `smem` bytes of dynamic shared memory (kThreads
+// threads).  A kernel's dynamic shared-memory limit is raised to the device's opt-in maximum
+// once, so that occupancy can be asked for several sizes (with and without carry slots) and any
+// of them launched.
 KernelInfo& kernel_info(const void* fn, size_t smem) {
     Engine& E = engine();
-    auto it = E.kinfo.find(fn);
-    if (it != E.kinfo.end() && it->second.smem == smem) return it->second;
+    const auto key = std::make_pair(fn, smem);
+    auto it = E.kinfo.find(key);
+    if (it != E.kinfo.end()) return it->second;
+    MCQ_REQUIRE(smem <= (size_t)E.smem_optin, MCQ_ERR_INTERNAL, "kernel shared memory above the device limit");
+    if (!E.kattr.count(fn)) {
+        MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, E.smem_optin));
+        E.kattr.insert(fn);
+    }
     KernelInfo ki;
     ki.smem = smem;
-    MCQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ki.blocks_per_sm, fn, kThreads, smem));
     MCQ_REQUIRE(ki.blocks_per_sm > 0, MCQ_ERR_INTERNAL, "kernel does not fit on an SM");
-    E.kinfo[fn] = ki;
-    return E.kinfo[fn];
+    return E.kinfo[key] = ki;
 }
 
 // The autotuner.  A family of kernels compiled with nvar launch variants that differ only in
@@ -503,9 +512,27 @@ void pass_async(Workspace& ws, const PassArgs& a, double* d_out) {
     const int skel = (a.noise == NOISE_BB && D > 32) ? ((D >> 5) + 1) * 32 : 0;
     const int accf = (!a.dump && a.est == EST_COUPLED && (k.model == MOD_BASKET || k.model == MOD_MULTI))
                          ? ((2 * nst + 3) & ~3) : 0;
-    const size_t smem = assist ? (size_t)kAssistTeams * kAssistTeamBytes
-                               : (size_t)kWarpsPerBlock * (1024 + skel + accf) * sizeof(float);
+    size_t smem = assist ? (size_t)kAssistTeams * kAssistTeamBytes
+                         : (size_t)kWarpsPerBlock * (1024 + skel + accf) * sizeof(float);
+    // Sobol start words carried from group to group of an item (one slot per tile a group
+    // generates): kept when an item has several groups and the slots leave the kernel's resident
+    // blocks per SM unchanged
+    k.carry = 0;
+    if (a.gen == GEN_SOBOL && !assist && !packed && gpi >= 2) {
+        int tiles = 0;
+        if (a.noise == NOISE_RAW) tiles = (D + 31) / 32;
+        else if ((a.noise == NOISE_BB || a.noise == NOISE_BB_UNI) && D > 32) tiles = ((D >> 5) + 31) / 32 + (D >> 5);
+        else if (a.noise == NOISE_BB || a.noise == NOISE_BB_UNI || knoise == NOISE_PCA) tiles = 1;
+        const size_t with = smem + (size_t)kWarpsPerBlock * 32 * tiles * sizeof(uint32_t);
+        if (tiles > 0 && with <= (size_t)E.smem_optin &&
+            kernel_info(fn, with).blocks_per_sm >= kernel_info(fn, smem).blocks_per_sm) {
+            k.carry = 32 * tiles;
+            smem = with;
+        }
+    }
     KernelInfo& ki = kernel_info(fn, smem);
+    E.last_gpi = k.gpi;
+    E.last_carry = k.carry;
     const int items_per_block = assist ? kAssistTeams : kWarpsPerBlock;
     long long blocks = ((long long)k.n_items + items_per_block - 1) / items_per_block;
     blocks = std::min<long long>(blocks, (long long)ki.blocks_per_sm * E.sm_count);

@@ -7,7 +7,9 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <map>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/mcq.h"
@@ -117,9 +119,12 @@ struct Engine {
     int sm_count = 148;
     uint32_t* d_dv = nullptr;                        // JoeKuo6 table [20000][32]
     std::vector<std::unique_ptr<Workspace>> pool;    // pool[0] is the default workspace
-    std::unordered_map<const void*, KernelInfo> kinfo;
+    int smem_optin = 227 * 1024;                     // dynamic shared memory a block may opt into
+    std::map<std::pair<const void*, size_t>, KernelInfo> kinfo;   // occupancy per (kernel, smem)
+    std::unordered_set<const void*> kattr;           // kernels whose smem limit is raised
     std::unordered_map<uint64_t, TuneState> tune;
     int launches = 0;                                // kernel launches issued (accounting)
+    int last_gpi = 0, last_carry = 0;                // work layout of the last fused pass
     Workspace& ws(int i);
 };
 

@@ -61,6 +61,7 @@ struct KParams {
     // ---- work split: R replicas x [offset, offset + n_points) points in 32-point groups
     int R;
     int gpi;            // groups per item
+    int carry;          // Sobol start-state words per warp in shared memory (0: walk every tile)
     int items_per_rep;
     int n_items;
     uint64_t offset;    // first point (Sobol index / Philox path id)

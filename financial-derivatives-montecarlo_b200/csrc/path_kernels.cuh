@@ -92,21 +92,34 @@ __device__ __forceinline__ void read_row(const float* buf, int lane, float (&z)[
 
 // Lane owns dimension `dim` of replica table `dr` (words [k * D + dim]); writes the normals of
 // points 32h .. 32h+31 into column `lane` of the transpose buffer.
+//
+// The start word x(32h) = shift ^ XOR of v_k over the set bits k of gray(32h), and
+// gray(32h) = gray(h) << 5 | (h & 1) << 4, so a tile walks popcount(gray(h)) words from the
+// digital shift.  A caller that generates the same dimension for groups h - 1, h, h + 1, ... in
+// order keeps the start word of each tile in `slot` (shared memory) and passes cont = true from
+// the second group on: x(32h) = x(32(h - 1)) ^ v_4 ^ v_{5 + ctz(h)}, two words instead of the
+// walk and its chain of dependent loads (the same word, so the same normals).
 __device__ __forceinline__ void sobol_tile(const uint32_t* __restrict__ dr, int D, int dim,
                                            bool active, uint64_t h, float u_cap, float* buf,
-                                           int lane) {
+                                           int lane, uint32_t* slot = nullptr, bool cont = false) {
     if (!active) return;
     const uint32_t* col = dr + dim;
     const uint32_t L0 = __ldg(col), L1 = __ldg(col + D), L2 = __ldg(col + 2 * D),
                    L3 = __ldg(col + 3 * D), L4 = __ldg(col + 4 * D);
-    uint32_t x = __ldg(col + 32 * D);
-    if (h & 1) x ^= L4;
-    uint32_t g = (uint32_t)(h ^ (h >> 1));
-    while (g) {
-        const int k = __ffs(g) - 1;
-        x ^= __ldg(col + (5 + k) * D);
-        g &= g - 1;
+    uint32_t x;
+    if (slot != nullptr && cont) {
+        x = *slot ^ L4 ^ __ldg(col + (4 + __ffsll((long long)h)) * D);
+    } else {
+        x = __ldg(col + 32 * D);
+        if (h & 1) x ^= L4;
+        uint32_t g = (uint32_t)(h ^ (h >> 1));
+        while (g) {
+            const int k = __ffs(g) - 1;
+            x ^= __ldg(col + (5 + k) * D);
+            g &= g - 1;
+        }
     }
+    if (slot != nullptr) *slot = x;
     // Four blocks of eight points: the gray-code step inside a block is compile-time (word
     // ctz(i + 1)), the step between blocks (points 8, 16, 24) XORs word 3 + ctz(b + 1).  Keeping
     // the block loop rolled holds the unrolled inverse-normal code to a quarter, which the
@@ -852,22 +865,27 @@ struct smem_tile_of { static constexpr bool value = false; };
 template <class C>
 struct smem_tile_of<C, std::void_t<decltype(C::SMEM_TILE)>> { static constexpr bool value = C::SMEM_TILE; };
 
+// One 32-path group h of a consumer.  `carry` (nullptr: none) holds the Sobol start words of
+// every tile the group generates, slot 32 t + lane for its t-th tile; cont says that the slots
+// hold group h - 1's words of the same replica (see sobol_tile).
 template <int GEN, int NOISE, class C>
 __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint32_t* dr,
                                           uint32_t stream, uint64_t h, uint64_t n, float* buf,
-                                          float* skel, int lane) {
+                                          float* skel, int lane, uint32_t* carry = nullptr,
+                                          bool cont = false) {
     const int D = p.D;
     if constexpr (NOISE == NOISE_RAW) {
         for (int d0 = 0; d0 < D; d0 += 32) {
             float z[32];
+            uint32_t* slot = carry ? carry + d0 + lane : nullptr;
             if constexpr (GEN == GEN_SOBOL && smem_tile_of<C>::value) {
-                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane, slot, cont);
                 __syncwarp();
                 cons.tile_smem(p, buf, lane, min(32, D - d0));
                 __syncwarp();
                 continue;
             } else if constexpr (GEN == GEN_SOBOL) {
-                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane, slot, cont);
                 __syncwarp();
                 read_row(buf, lane, z);
                 __syncwarp();
@@ -880,7 +898,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         // N <= 32 (one tile): dW_i = sum_k M[i][k] z_k with z and M rounded to fp16 as the
         // reference's cast + GEMM (methods_cuda.cu:1228-1229); larger N runs in k_pca.
         const int N = D;
-        sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane);
+        sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane, carry ? carry + lane : nullptr, cont);
         __syncwarp();
         float z[32];
         read_row(buf, lane, z);
@@ -915,7 +933,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         const int N = D;
         if (N <= 32) {
             // one tile: the literal table-driven bridge (bb_apply, utils.cpp:104-124)
-            sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane);
+            sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane, carry ? carry + lane : nullptr, cont);
             __syncwarp();
             float z[32];
             read_row(buf, lane, z);
@@ -940,8 +958,11 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
             // per lane in shared memory at skel[q * 32 + lane]; then S windows of 32 steps.
             const int S = N >> 5;
             skel[lane] = 0.f;
+            // carry slots: the skeleton tiles first, then one per window
+            const int ns = (S + 31) & ~31;
             for (int t0 = 0; t0 < S; t0 += 32) {
-                sobol_tile(dr, p.dstride, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane,
+                           carry ? carry + t0 + lane : nullptr, cont);
                 __syncwarp();
                 float z[32];
                 read_row(buf, lane, z);
@@ -965,7 +986,8 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
                     const int u = 31 - __clz(lane + 1);
                     dim = (S << u) + (q << u) + (lane + 1 - (1 << u));
                 }
-                sobol_tile(dr, p.dstride, dim, act, h, p.u_cap, buf, lane);
+                sobol_tile(dr, p.dstride, dim, act, h, p.u_cap, buf, lane,
+                           carry ? carry + ns + 32 * q + lane : nullptr, cont);
                 __syncwarp();
                 float z[32];
                 read_row(buf, lane, z);
@@ -1111,9 +1133,10 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : (noise_is_bb(NOISE) ? 
     constexpr bool WACC = warp_acc_of<C>::value;
     const int skel_floats = (noise_is_bb(NOISE) && p.D > 32) ? ((p.D >> 5) + 1) * 32 : 0;
     const int acc_floats = WACC ? ((2 * C::NST + 3) & ~3) : 0;
-    float* buf = reinterpret_cast<float*>(smem4) + wib * (1024 + skel_floats + acc_floats);
+    float* buf = reinterpret_cast<float*>(smem4) + wib * (1024 + skel_floats + acc_floats + p.carry);
     float* skel = buf + 1024;
     double* wrec = reinterpret_cast<double*>(buf + 1024 + skel_floats);
+    uint32_t* carry = p.carry ? reinterpret_cast<uint32_t*>(buf + 1024 + skel_floats + acc_floats) : nullptr;
     const int total_warps = gridDim.x * kWarpsPerBlock;
     const uint64_t gend_all = p.g0 + p.G;
     for (int item = blockIdx.x * kWarpsPerBlock + wib; item < p.n_items; item += total_warps) {
@@ -1161,7 +1184,7 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : (noise_is_bb(NOISE) ? 
                 cons.init(p);
                 if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
                 else cons.bind(r, n);
-                run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane);
+                run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane, carry, h != gb);
                 float y[C::NST];
                 cons.finish(p, y);
                 const bool valid = n >= p.offset && n < p.offset + p.n_points;
