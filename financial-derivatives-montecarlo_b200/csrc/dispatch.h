@@ -8,9 +8,10 @@ namespace mcq {
 
 const void* lookup_sobol_raw_plain(int model, int payoff);
 const void* lookup_sobol_raw_plain_b4(int model, int payoff);   // 64-register variant
-const void* lookup_sobol_raw_plain_b5(int model, int payoff);   // 48-register variant
+const void* lookup_sobol_raw_plain_u4(int model, int payoff);   // 64 registers, unrolled tile
 const void* lookup_sobol_raw_coupled(int model, int payoff);
 const void* lookup_sobol_raw_coupled_b4(int model, int payoff);   // 64-register variant
+const void* lookup_sobol_raw_coupled_u4(int model, int payoff);   // 64 registers, unrolled tile
 const void* lookup_sobol_packed(int model, int payoff, bool coupled);   // raw, D <= 16 (NOISE_PACKED)
 const void* lookup_assist(int gen, int model, int payoff, bool coupled);  // raw, few long paths (NOISE_ASSIST)
 const void* lookup_sobol_bb(int model, int payoff, bool coupled);
@@ -26,7 +27,7 @@ const void* lookup_misc(int gen, int noise, int est, int model, int nb, bool dum
 // Kernel families with more than one compiled launch variant (see the autotuner in engine.cpp).
 inline int n_variants(int gen, int noise, int est, int model) {
     if (gen != GEN_SOBOL || model == MOD_MULTI || model == MOD_BASKET) return 1;
-    if (est == EST_COUPLED) return (noise == NOISE_RAW && model != MOD_LVGRID) ? 2 : 1;
+    if (est == EST_COUPLED) return (noise == NOISE_RAW && model != MOD_LVGRID) ? 3 : 1;
     if (est != EST_PLAIN) return 1;
     if (noise == NOISE_RAW) return 3;
     if (noise == NOISE_BB && model != MOD_HESTON) return 2;
@@ -35,9 +36,11 @@ inline int n_variants(int gen, int noise, int est, int model) {
 }
 inline const void* lookup_variant(int gen, int noise, int est, int model, int payoff, int variant) {
     if (variant < 1 || variant >= n_variants(gen, noise, est, model)) return nullptr;
-    if (est == EST_COUPLED) return lookup_sobol_raw_coupled_b4(model, payoff);
+    if (est == EST_COUPLED)
+        return variant == 1 ? lookup_sobol_raw_coupled_b4(model, payoff) : lookup_sobol_raw_coupled_u4(model, payoff);
     if (noise == NOISE_BB_UNI) return lookup_sobol_bbu(model, payoff, false, variant);
-    if (noise == NOISE_RAW) return variant == 1 ? lookup_sobol_raw_plain_b4(model, payoff) : lookup_sobol_raw_plain_b5(model, payoff);
+    if (noise == NOISE_RAW)
+        return variant == 1 ? lookup_sobol_raw_plain_b4(model, payoff) : lookup_sobol_raw_plain_u4(model, payoff);
     return lookup_sobol_bb_b3(model, payoff);
 }
 

@@ -5,16 +5,16 @@
 
 namespace mcq {
 
-template <int GEN, int NOISE, int MOD, bool CPL, int MINB = 0>
+template <int GEN, int NOISE, int MOD, bool CPL, int MINB = 0, int GU = 1>
 const void* pick_payoff(int pay) {
     switch (pay) {
         case PAY_EUR:
-        case PAY_BASKET: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_EUR, CPL>, MINB>;
-        case PAY_ASIAN: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_ASIAN, CPL>, MINB>;
-        case PAY_GEOM: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_GEOM, CPL>, MINB>;
-        case PAY_LOOKBACK: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_LOOKBACK, CPL>, MINB>;
-        case PAY_UPOUT: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_UPOUT, CPL>, MINB>;
-        case PAY_DOWNOUT: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_DOWNOUT, CPL>, MINB>;
+        case PAY_BASKET: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_EUR, CPL>, MINB, GU>;
+        case PAY_ASIAN: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_ASIAN, CPL>, MINB, GU>;
+        case PAY_GEOM: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_GEOM, CPL>, MINB, GU>;
+        case PAY_LOOKBACK: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_LOOKBACK, CPL>, MINB, GU>;
+        case PAY_UPOUT: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_UPOUT, CPL>, MINB, GU>;
+        case PAY_DOWNOUT: return (const void*)&k_pass<GEN, NOISE, PathC<MOD, PAY_DOWNOUT, CPL>, MINB, GU>;
         default: return nullptr;
     }
 }

@@ -153,8 +153,7 @@ __device__ __forceinline__ void sobol_tile_to_A(const uint32_t* __restrict__ dr,
             *reinterpret_cast<__half*>(base + r * 128 + ((chunk ^ (r & 7)) << 4)) =
                 __float2half_rn(sobol_normal(x, u_cap));
             if (i < 7) {
-                const int c = cx_ctz(i + 1);
-                x ^= (c == 0) ? L0 : (c == 1) ? L1 : L2;
+                x ^= gray_word8(i, L0, L1, L2);
             } else if (b < 3) {
                 x ^= (b == 1) ? L4 : L3;
             }

@@ -173,10 +173,26 @@ static void qmc_pass_noalloc(const mcq_model* m, const mcq_payoff* p, int n_step
     k.dirs = dirs;
     k.partials = partials;
 
-    const size_t smem = (size_t)kWarpsPerBlock * 1024 * sizeof(float);
+    size_t smem = (size_t)kWarpsPerBlock * 1024 * sizeof(float);
     int per_sm = 0;
     MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
     MCQ_REQUIRE(per_sm > 0, MCQ_ERR_INTERNAL, "kernel does not fit on an SM");
+    // Sobol start words carried from group to group (one slot per 32-dimension tile), as the
+    // allocating pass does: when items hold several groups, the slots stay within the default
+    // 48 KB of dynamic shared memory (no attribute change) and keep the resident blocks per SM
+    k.carry = 0;
+    if (!packed && gpi >= 2) {
+        const int words = 32 * ((D + 31) / 32);
+        const size_t with = smem + (size_t)kWarpsPerBlock * words * sizeof(uint32_t);
+        int per_sm_c = 0;
+        if (with <= 48 * 1024) {
+            MCQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, fn, kThreads, with));
+            if (per_sm_c >= per_sm) {
+                k.carry = words;
+                smem = with;
+            }
+        }
+    }
     long long blocks = ((long long)k.n_items + kWarpsPerBlock - 1) / kWarpsPerBlock;
     blocks = std::min<long long>(blocks, (long long)per_sm * sms);
     blocks = std::max<long long>(blocks, 1);

@@ -38,7 +38,13 @@ constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kTwoPow32Inv = 2.3283064365386963e-10f;   // 2^-32
 constexpr float kTwoPow24Inv = 5.9604644775390625e-08f;   // 2^-24
 
-__host__ __device__ constexpr int cx_ctz(int v) { return (v & 1) ? 0 : 1 + cx_ctz(v >> 1); }
+// Direction word of the gray-code step from point i to point i + 1 inside a block of eight
+// (i = 0..6: word ctz(i + 1) = 0, 1, 0, 2, 0, 1, 0), written as bit tests of i so that an unrolled
+// i folds to one XOR operand.  (A recursive constexpr ctz called with the loop index is not
+// folded by the device compiler: it left ~10 integer and branch instructions per normal.)
+__device__ __forceinline__ uint32_t gray_word8(int i, uint32_t L0, uint32_t L1, uint32_t L2) {
+    return (i & 1) == 0 ? L0 : ((i & 2) ? L2 : L1);
+}
 
 // ------------------------------------------------------------------ hashing / scrambling
 
@@ -99,9 +105,27 @@ __device__ __forceinline__ void read_row(const float* buf, int lane, float (&z)[
 // order keeps the start word of each tile in `slot` (shared memory) and passes cont = true from
 // the second group on: x(32h) = x(32(h - 1)) ^ v_4 ^ v_{5 + ctz(h)}, two words instead of the
 // walk and its chain of dependent loads (the same word, so the same normals).
+//
+// The 32 points run as four blocks of eight: inside a block the gray-code step is fixed (word
+// ctz(i + 1), gray_word8), between blocks (points 8, 16, 24) it XORs word 3 + ctz(b + 1).  UNR
+// blocks are unrolled at a time (1, 2 or 4): a larger unroll drops the loop's overhead but
+// multiplies the inlined inverse-normal code the instruction cache must hold; the fused pass
+// families are compiled with more than one and the autotuner picks (the same normals).
+__device__ __forceinline__ void sobol_block8(uint32_t& x, int b, uint32_t L0, uint32_t L1, uint32_t L2,
+                                             uint32_t L3, uint32_t L4, float u_cap, float* buf, int lane) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        buf[swz(8 * b + i, lane)] = sobol_normal(x, u_cap);
+        if (i < 7) x ^= gray_word8(i, L0, L1, L2);
+        else if (b < 3) x ^= (b == 1) ? L4 : L3;
+    }
+}
+
+template <int UNR = 1>
 __device__ __forceinline__ void sobol_tile(const uint32_t* __restrict__ dr, int D, int dim,
                                            bool active, uint64_t h, float u_cap, float* buf,
                                            int lane, uint32_t* slot = nullptr, bool cont = false) {
+    static_assert(UNR == 1 || UNR == 2 || UNR == 4, "blocks unrolled: 1, 2 or 4");
     if (!active) return;
     const uint32_t* col = dr + dim;
     const uint32_t L0 = __ldg(col), L1 = __ldg(col + D), L2 = __ldg(col + 2 * D),
@@ -120,22 +144,15 @@ __device__ __forceinline__ void sobol_tile(const uint32_t* __restrict__ dr, int 
         }
     }
     if (slot != nullptr) *slot = x;
-    // Four blocks of eight points: the gray-code step inside a block is compile-time (word
-    // ctz(i + 1)), the step between blocks (points 8, 16, 24) XORs word 3 + ctz(b + 1).  Keeping
-    // the block loop rolled holds the unrolled inverse-normal code to a quarter, which the
-    // instruction cache keeps resident: ~1.35x on the book kernel against a 32-point unroll.
-#pragma unroll 1
-    for (int b = 0; b < 4; b++) {
+    if constexpr (UNR == 4) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            buf[swz(8 * b + i, lane)] = sobol_normal(x, u_cap);
-            if (i < 7) {
-                const int c = cx_ctz(i + 1);
-                x ^= (c == 0) ? L0 : (c == 1) ? L1 : L2;
-            } else if (b < 3) {
-                x ^= (b == 1) ? L4 : L3;
-            }
-        }
+        for (int b = 0; b < 4; b++) sobol_block8(x, b, L0, L1, L2, L3, L4, u_cap, buf, lane);
+    } else if constexpr (UNR == 2) {
+#pragma unroll 2
+        for (int b = 0; b < 4; b++) sobol_block8(x, b, L0, L1, L2, L3, L4, u_cap, buf, lane);
+    } else {
+#pragma unroll 1
+        for (int b = 0; b < 4; b++) sobol_block8(x, b, L0, L1, L2, L3, L4, u_cap, buf, lane);
     }
 }
 
@@ -868,7 +885,7 @@ struct smem_tile_of<C, std::void_t<decltype(C::SMEM_TILE)>> { static constexpr b
 // One 32-path group h of a consumer.  `carry` (nullptr: none) holds the Sobol start words of
 // every tile the group generates, slot 32 t + lane for its t-th tile; cont says that the slots
 // hold group h - 1's words of the same replica (see sobol_tile).
-template <int GEN, int NOISE, class C>
+template <int GEN, int NOISE, class C, int GU = 1>
 __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint32_t* dr,
                                           uint32_t stream, uint64_t h, uint64_t n, float* buf,
                                           float* skel, int lane, uint32_t* carry = nullptr,
@@ -879,13 +896,13 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
             float z[32];
             uint32_t* slot = carry ? carry + d0 + lane : nullptr;
             if constexpr (GEN == GEN_SOBOL && smem_tile_of<C>::value) {
-                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane, slot, cont);
+                sobol_tile<GU>(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane, slot, cont);
                 __syncwarp();
                 cons.tile_smem(p, buf, lane, min(32, D - d0));
                 __syncwarp();
                 continue;
             } else if constexpr (GEN == GEN_SOBOL) {
-                sobol_tile(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane, slot, cont);
+                sobol_tile<GU>(dr, p.dstride, d0 + lane, d0 + lane < D, h, p.u_cap, buf, lane, slot, cont);
                 __syncwarp();
                 read_row(buf, lane, z);
                 __syncwarp();
@@ -898,7 +915,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         // N <= 32 (one tile): dW_i = sum_k M[i][k] z_k with z and M rounded to fp16 as the
         // reference's cast + GEMM (methods_cuda.cu:1228-1229); larger N runs in k_pca.
         const int N = D;
-        sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane, carry ? carry + lane : nullptr, cont);
+        sobol_tile<GU>(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane, carry ? carry + lane : nullptr, cont);
         __syncwarp();
         float z[32];
         read_row(buf, lane, z);
@@ -933,7 +950,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
         const int N = D;
         if (N <= 32) {
             // one tile: the literal table-driven bridge (bb_apply, utils.cpp:104-124)
-            sobol_tile(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane, carry ? carry + lane : nullptr, cont);
+            sobol_tile<GU>(dr, p.dstride, lane, lane < N, h, p.u_cap, buf, lane, carry ? carry + lane : nullptr, cont);
             __syncwarp();
             float z[32];
             read_row(buf, lane, z);
@@ -961,7 +978,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
             // carry slots: the skeleton tiles first, then one per window
             const int ns = (S + 31) & ~31;
             for (int t0 = 0; t0 < S; t0 += 32) {
-                sobol_tile(dr, p.dstride, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane,
+                sobol_tile<GU>(dr, p.dstride, t0 + lane, t0 + lane < S, h, p.u_cap, buf, lane,
                            carry ? carry + t0 + lane : nullptr, cont);
                 __syncwarp();
                 float z[32];
@@ -986,7 +1003,7 @@ __device__ __forceinline__ void run_group(const KParams& p, C& cons, const uint3
                     const int u = 31 - __clz(lane + 1);
                     dim = (S << u) + (q << u) + (lane + 1 - (1 << u));
                 }
-                sobol_tile(dr, p.dstride, dim, act, h, p.u_cap, buf, lane,
+                sobol_tile<GU>(dr, p.dstride, dim, act, h, p.u_cap, buf, lane,
                            carry ? carry + ns + 32 * q + lane : nullptr, cont);
                 __syncwarp();
                 float z[32];
@@ -1121,7 +1138,7 @@ struct warp_acc_of { static constexpr bool value = false; };
 template <int MOD, int NB>
 struct warp_acc_of<BasketLevelC<MOD, NB>> { static constexpr bool value = true; };
 
-template <int GEN, int NOISE, class C, int MINB = 0>
+template <int GEN, int NOISE, class C, int MINB = 0, int GU = 1>
 __global__ void __launch_bounds__(kThreads, MINB ? MINB : (noise_is_bb(NOISE) ? 2 : kMinBlocks))
     k_pass(const __grid_constant__ KParams p) {
     extern __shared__ float4 smem4[];
@@ -1184,7 +1201,7 @@ __global__ void __launch_bounds__(kThreads, MINB ? MINB : (noise_is_bb(NOISE) ? 
                 cons.init(p);
                 if constexpr (std::is_same<C, DumpC>::value) cons.bind(p, r, n);
                 else cons.bind(r, n);
-                run_group<GEN, NOISE>(p, cons, dr, stream, h, n, buf, skel, lane, carry, h != gb);
+                run_group<GEN, NOISE, C, GU>(p, cons, dr, stream, h, n, buf, skel, lane, carry, h != gb);
                 float y[C::NST];
                 cons.finish(p, y);
                 const bool valid = n >= p.offset && n < p.offset + p.n_points;
