@@ -656,10 +656,11 @@ def main():
                                      "frac": achieved * ISSUE_MODEL_FLOPS_PER_PATH_STEP / FLOPS_PER_PATH_STEP / peak_fp32,
                                      "what": "the inverse normal counted as the 29-flop AS241 rational"},
                      "issue_active_ncu": issue,
+                     "instructions_per_path_step_ncu": 37.7,
                      "note": "instruction-issue bound: the algorithmic count is 13 FP32 flops and one inverse "
-                             "normal per path-step, the kernel issues about 49 thread instructions per path-step "
-                             "(Sobol gray-code integer work, conversions, the inverse normal's own instructions, "
-                             "transposes) at the issue activity of the committed ncu capture"},
+                             "normal per path-step, the kernel issues about 38 thread instructions per path-step "
+                             "(about 24 in CUDA's normcdfinvf, 3 in the GBM step and Asian sum, 10 in the Sobol "
+                             "generation and transpose) at the issue activity of the committed ncu capture"},
         "gpu_launches": 2 * args.steps,
         "clocks": clocks,
     }

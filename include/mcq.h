@@ -344,8 +344,9 @@ int mcq_is_pass(const mcq_model* m, const mcq_payoff* p, int n_steps, double z_s
  * device.  Its scratch is one fixed __device__ array inside the library (about 2.7 MiB, held on
  * every GPU that loads the library until exit); sums_device ([R][2] doubles) is the caller's.
  * Limits: GBM, Heston or parametric Dupire, raw ordering, n_steps x factors <= 512, R <= 32;
- * larger requests fail with MCQ_ERR_RANGE.  Same kernel and work split as mcq_qmc_pass_device,
- * hence the same sums bit for bit.  The first call on a device (and the first in a new context of
+ * larger requests fail with MCQ_ERR_RANGE.  Same kernel family, work split and carried Sobol
+ * start words as mcq_qmc_pass_device (in one of the family's launch variants, which all give
+ * the same bits), hence the same sums bit for bit.  The first call on a device (and the first in a new context of
  * it, e.g. after cudaDeviceReset) loads the direction table into the array with a synchronous
  * copy and should come before any stream capture.  All calls share the array: calls that
  * overlap on the GPU race, so keep them on one stream.  Asynchronous on `stream` (NULL: the
