@@ -269,12 +269,13 @@ def book_checks(eng, opts, res, orv, first_index=0):
     return out
 
 
-def book_bench(eng, n, n_loose, orv):
+def book_bench(eng, n, n_loose, orv, n_all=0):
     """The batched heterogeneous book against its plain form on the same GPU: the first n options
     of the 4096-option synthetic book (d ~ U{1..16}, correlated GBM, Dirichlet weights, T ~
     U[0.1, 3], 16-512 finest steps, eps ~ U[5e-4, 5e-3]), each priced by MLQMC (R = 16, M = 2)
     with its per-asset pathwise deltas: at each option's own eps, at the metric's eps = 1e-3 for
-    every option, and (the first n_loose options) at the loosest eps of the range, 5e-3.  Each mode
+    every option, and (the first n_loose options) at the loosest eps of the range, 5e-3; the first
+    n_all options at eps = 1e-3 in the batched form only (the full-size configuration).  Each mode
     is timed by the library around its pricing loop (host wall time with the device
     synchronised), after a warm-up book.  Under torchrun the options are dealt round-robin over the
     ranks (the same n in total) and the time is the maximum over ranks."""
@@ -325,10 +326,36 @@ def book_bench(eng, n, n_loose, orv):
             out.append(c)
         return out
 
+    def batched_only(opts, total):
+        r, st = eng.book_price(opts, eng.BOOK_BATCHED) if opts else ([], {"time_s": 0.0, "rounds": 0, "launches": 0,
+                                                                         "normals": 0.0, "path_steps": 0.0})
+        agg = torch.tensor([st["time_s"], st["normals"], st["path_steps"]], dtype=torch.float64, device="cuda")
+        if world > 1:
+            t = agg[:1].clone()
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            w = agg[1:].clone()
+            torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+            agg = torch.cat([t, w])
+        tmax, normals, psteps = agg.tolist()
+        d = {"options": total, "batched": {"options_per_s": total / tmax, "time_s": tmax, "rounds": st["rounds"],
+                                           "launches": st["launches"], "normals_per_s": normals / tmax,
+                                           "path_steps_per_s": psteps / tmax}}
+        d["non_finite"] = sum(1 for a in r if not math.isfinite(a["price"]))
+        d["checks"] = book_checks(eng, opts, r, orv) if world == 1 else None
+        d["converged"] = sum(1 for x in r if x["converged"])
+        return d
+
     mine = [book[i] for i in range(rank, n, world)]
     out = {"options": n, "workload": "first %d of the 4096-option synthetic basket book (seed 5), %.1f %% of it; "
                                      "MLQMC R=16 M=2 n0=1, price + per-asset delta" % (n, 100.0 * n / 4096),
            "sharding": "options round-robin over %d rank(s), fixed total" % world}
+    if n_all > 0:
+        # the metric's configuration at (up to) its full size: every option at eps = 1e-3, batched form only
+        # (the plain form of all 4096 would double the section's minutes; its ratio is measured on the prefix)
+        all_mine = [book[i] for i in range(rank, n_all, world)]
+        out["eps_1e-3_all"] = batched_only(at_eps(all_mine, 1e-3), n_all)
+        out["eps_1e-3_all"]["workload"] = ("first %d of the 4096-option book (%.1f %% of it) at eps = 1e-3, batched"
+                                           % (n_all, 100.0 * n_all / 4096))
     out["eps_1e-3"] = both_modes(at_eps(mine, 1e-3), n)
     out["own_eps"] = both_modes(mine, n)
     loose = [book[i] for i in range(rank, n_loose, world)]
@@ -434,6 +461,8 @@ def main():
                     help="options of the synthetic basket book priced batched and plain (0: skip)")
     ap.add_argument("--book-options-loose", type=int, default=4096,
                     help="options priced at the loosest eps of the range (5e-3)")
+    ap.add_argument("--book-options-all", type=int, default=4096,
+                    help="options priced batched only at the metric's eps = 1e-3 (0: skip)")
     ap.add_argument("--no-configs", action="store_true", help="skip the MC / Heston MLQMC / adjoint workloads")
     ap.add_argument("--book-slice", default=None, metavar="D:LEVEL[:POINTS]",
                     help="only price one slice of a D-asset basket at LEVEL through the book kernel "
@@ -589,7 +618,8 @@ def main():
     h2d_e2e = ctypes.sizeof(m) + ctypes.sizeof(p) + ctypes.sizeof(cfg)
 
     orv = oracle_values()
-    book = None if args.book_options <= 0 else book_bench(eng, args.book_options, args.book_options_loose, orv)
+    book = None if args.book_options <= 0 else book_bench(eng, args.book_options, args.book_options_loose, orv,
+                                                          args.book_options_all)
     others = None if args.no_configs else configs_bench(eng, orv)
 
     if world > 1:

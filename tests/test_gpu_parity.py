@@ -156,25 +156,28 @@ def test_launch_variants_are_bit_identical(gpu, model, pay):
     try:
         for v in ("0", "1", "2"):
             os.environ["MCQ_TUNE"] = v
-            out.append(gpu.qmc_pass(m, p, 64, salt_base=42, R=4, offset=3, n_points=50000))
+            out.append(gpu.qmc_pass(m, p, 64, salt_base=42, R=4, offset=3, n_points=400000))
     finally:
         os.environ.pop("MCQ_TUNE", None)
+    assert gpu.debug_last_pass_layout()[0] >= 2   # items of several groups: carried start words in play
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
 @pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("heston", "lookback"), ("dupire", "eur")])
 def test_coupled_launch_variants_are_bit_identical(gpu, model, pay):
-    """The coupled MLMC / MLQMC level pass under its two register budgets."""
+    """The coupled MLMC / MLQMC level pass under its three launch variants (two register budgets,
+    and the unrolled tile generator)."""
     import os
     m, p = make_model(gpu, model), make_payoff(gpu, pay)
     out = []
     try:
-        for v in ("0", "1"):
+        for v in ("0", "1", "2"):
             os.environ["MCQ_TUNE"] = v
-            out.append(gpu.level_pass(m, p, 64, 4, use_sobol=True, salt_base=42, R=4, offset=3, n_points=50000))
+            out.append(gpu.level_pass(m, p, 64, 4, use_sobol=True, salt_base=42, R=4, offset=3, n_points=400000))
     finally:
         os.environ.pop("MCQ_TUNE", None)
-    assert np.array_equal(out[0], out[1])
+    assert gpu.debug_last_pass_layout()[0] >= 2
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
 @pytest.mark.parametrize("model,pay", [("gbm", "asian"), ("dupire", "eur")])
@@ -186,10 +189,11 @@ def test_bridge_launch_variants_are_bit_identical(gpu, model, pay):
     try:
         for v in ("0", "1", "2"):   # a uniform time grid: the window weights come from the parameters
             os.environ["MCQ_TUNE"] = v
-            out.append(gpu.qmc_pass(m, p, 256, noise=gpu.BB, bb=bb, salt_base=42, R=4, offset=3, n_points=20000))
+            out.append(gpu.qmc_pass(m, p, 256, noise=gpu.BB, bb=bb, salt_base=42, R=4, offset=3, n_points=320000))
     finally:
         os.environ.pop("MCQ_TUNE", None)
         bb.close()
+    assert gpu.debug_last_pass_layout()[0] >= 2
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
