@@ -150,9 +150,9 @@ static void qmc_pass_noalloc(const mcq_model* m, const mcq_payoff* p, int n_step
     const void* fn = (D <= 16) ? lookup_sobol_packed(k.model, p->kind, false) : nullptr;
     const bool packed = fn != nullptr;
     // the plain pass in the launch variant the autotuner keeps for these families on a B200 (it does
-    // not run here: no timing events on the caller's stream): the unrolled tile generator for GBM and
-    // Heston, the 64-register rolled one for Dupire (all variants give the same bits)
-    if (!fn) fn = lookup_variant(GEN_SOBOL, NOISE_RAW, EST_PLAIN, k.model, p->kind, k.model == MOD_DUPIRE ? 1 : 2);
+    // not run here: no timing events on the caller's stream): the unrolled tile generator (all
+    // variants give the same bits)
+    if (!fn) fn = lookup_variant(GEN_SOBOL, NOISE_RAW, EST_PLAIN, k.model, p->kind, 2);
     if (!fn) fn = lookup_pass(GEN_SOBOL, NOISE_RAW, EST_PLAIN, k.model, p->kind, 0);
     MCQ_REQUIRE(fn != nullptr, MCQ_ERR_UNSUPPORTED, "no fused kernel for this model / payoff");
     const uint64_t g0 = a.offset >> 5;

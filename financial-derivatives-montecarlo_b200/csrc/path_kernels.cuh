@@ -279,6 +279,19 @@ __device__ __forceinline__ float sqrt_approx(float v) {
     return r;
 }
 
+// Parametric Dupire local volatility sigma0 e^{-alpha t} (S/S0)^(beta - 1) = sigma0 2^{(beta - 1) log2(S/S0)
+// - alpha t log2(e)}, x = S/S0, with the hardware's approximate base-2 logarithm and exponential
+// (`lg2.approx.f32`, `ex2.approx.f32`: errors about 2^-22, the same special values: log2 of 0 is
+// -inf, of a negative x NaN, 2^-inf = 0).  As with the Heston square root, the error scales the
+// volatility (1 +- 1e-6), which multiplies only the mean-zero increment: it biases no drift.
+__device__ __forceinline__ float dupire_vol(const KParams& p, float x, float t) {
+    float l, e;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(l) : "f"(x));
+    const float a = fmaf(p.bm1, l, -p.alpha * t * kLog2e);
+    asm("ex2.approx.f32 %0, %1;" : "=f"(e) : "f"(a));
+    return p.sigma0 * e;
+}
+
 template <int PAY>
 __host__ __device__ constexpr bool path_dep() {
     return PAY == PAY_ASIAN || PAY == PAY_GEOM || PAY == PAY_LOOKBACK || PAY == PAY_UPOUT ||
@@ -323,7 +336,7 @@ struct Leg {
         if constexpr (MOD == MOD_GBM) {
             S = fmaf(S, fmaf(p.sigma, dw1, muh), S);
         } else if constexpr (MOD == MOD_DUPIRE) {
-            const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S * p.inv_S0), -p.alpha * t * kLog2e));
+            const float sl = dupire_vol(p, S * p.inv_S0, t);
             S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_LVGRID) {
             const float sl = lv_sigma(p, S, t);
@@ -527,7 +540,7 @@ struct CvDupireC {
     }
     __device__ __forceinline__ void step_dw(const KParams& p, float dw, float) {
         const float t = (float)k * p.h;
-        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(Sd * p.inv_S0), -p.alpha * t * kLog2e));
+        const float sl = dupire_vol(p, Sd * p.inv_S0, t);
         Sd = fmaf(Sd, fmaf(sl, dw, muh), Sd);
         Sg = fmaf(Sg, fmaf(p.ctrl_sigma, dw, muh), Sg);
         k++;
@@ -611,8 +624,7 @@ struct BasketC {
             for (int a = 0; a < NB; a++) {
                 if (a < n) {
                     if constexpr (MOD == MOD_MULTI) {
-                        const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * __ldg(p.bsk + n + a)),
-                                                               -p.alpha * t * kLog2e));
+                        const float sl = dupire_vol(p, S[a] * __ldg(p.bsk + n + a), t);
                         S[a] = fmaf(S[a], fmaf(sl, dw[a], muh), S[a]);
                     } else {
                         S[a] = fmaf(S[a], fmaf(__ldg(p.bsk + n + a), dw[a], muh), S[a]);
@@ -707,7 +719,7 @@ struct BasketLevelC {
     // sigma_loc(S, t) S-scale: the per-asset inverse reference S0 (second block of p.bsk)
     __device__ __forceinline__ float vol(const KParams& p, int n, int a, float S, float t) const {
         if constexpr (MOD == MOD_MULTI)
-            return p.sigma0 * exp2f(fmaf(p.bm1, log2f(S * __ldg(p.bsk + n + a)), -p.alpha * t * kLog2e));
+            return dupire_vol(p, S * __ldg(p.bsk + n + a), t);
         else
             return __ldg(p.bsk + n + a);
     }
@@ -819,8 +831,7 @@ struct BasketWideC {
 #pragma unroll 1
             for (int a = 0; a < n; a++) {
                 if constexpr (MOD == MOD_MULTI) {
-                    const float sl = p.sigma0 * exp2f(fmaf(p.bm1, log2f(S[a] * __ldg(p.bsk + n + a)),
-                                                           -p.alpha * t * kLog2e));
+                    const float sl = dupire_vol(p, S[a] * __ldg(p.bsk + n + a), t);
                     S[a] = fmaf(S[a], fmaf(sl, dw[a], muh), S[a]);
                 } else {
                     S[a] = fmaf(S[a], fmaf(__ldg(p.bsk + n + a), dw[a], muh), S[a]);
