@@ -144,8 +144,8 @@ __device__ __forceinline__ void sobol_tile_to_A(const uint32_t* __restrict__ dr,
     }
     unsigned char* base = A + (e & 7) * 2;
     const int chunk = e >> 3;
-    // four blocks of eight points, the block loop rolled (the gray-code steps as in sobol_tile)
-#pragma unroll 1
+    // four blocks of eight points (the gray-code steps as in sobol_tile), unrolled
+#pragma unroll
     for (int b = 0; b < 4; b++) {
 #pragma unroll
         for (int i = 0; i < 8; i++) {
