@@ -501,14 +501,14 @@ def main():
     sp = stream.cuda_stream
     assert sp != 0
 
-    gsums = torch.zeros(world * REPS * 2, dtype=torch.float64, device="cuda") if world > 1 else sums
+    import importlib
+    sharded = importlib.import_module("fdmc_b200.sharded")
+    gsums = [sums]   # the estimator's [32 N][2] per-replica sums after the last pass
 
     def one_pass():
         eng.qmc_pass_device(m, p, STEPS, sums.data_ptr(), sp, salt_base=salt, R=REPS, offset=0, n_points=N)
         if world > 1:   # the estimator over all ranks' replicas, on every rank (NCCL on `stream`)
-            gsums.zero_()
-            gsums[rank * REPS * 2:(rank + 1) * REPS * 2].copy_(sums)
-            torch.distributed.all_reduce(gsums, op=torch.distributed.ReduceOp.SUM)
+            gsums[0] = sharded.combine_replica_sums(sums.view(REPS, 2), world * REPS)
 
     # the clock sampler starts before the warm-up (nvidia-smi needs a moment to start) and its
     # summary keeps the samples from the start of the timed region on
@@ -543,7 +543,7 @@ def main():
         total_ms = float(t.item())
     ps_per_step = REPS * N * STEPS
     value = world * ps_per_step * args.steps / (total_ms * 1e-3)
-    chk = gsums.cpu().numpy().reshape(world * REPS, 2)
+    chk = gsums[0].cpu().numpy().reshape(world * REPS, 2)
     rmeans = chk[:, 0] / N
     price = float(rmeans.mean())
     price_se = float(rmeans.std(ddof=1) / math.sqrt(world * REPS))
@@ -588,9 +588,6 @@ def main():
             r = eng.run_qmc(m, p, 1e-3, STEPS, cfg)
             return r, r["path_steps"]
     else:
-        import importlib
-        sharded = importlib.import_module("fdmc_b200.sharded")
-
         def e2e_run():
             def pass_fn(r0, nr, offset, n):
                 return eng.qmc_pass(m, p, STEPS, salt_base=SALT + r0, R=nr, offset=offset, n_points=n)

@@ -3,6 +3,9 @@
 The RQMC estimator is a mean over R independently scrambled replicas, and a book is a list of
 independent options, so the path shards without any exchange inside a pass:
 
+* `combine_replica_sums` — the one exchange of a replica-split estimator: each rank's block of
+  per-replica sums into the [R][k] sums of all replicas on every rank (one all-reduce, one
+  contributor per slot, so bit for bit).  The multi-GPU benchmark uses it after every pass.
 * `run_qmc_sharded` — the doubling loop of run_qmc_cuda (methods_cuda.cu:1624-1668) with the R
   replicas split into contiguous blocks, one per rank (replica r keeps salt salt_base + r, so the
   points are those of the one-process run).  After each doubling the per-replica sums are
@@ -43,6 +46,25 @@ def replica_block(R, world, rank):
     return R * rank // world, R * (rank + 1) // world
 
 
+def combine_replica_sums(local, R, group=None):
+    """The estimator's per-replica sums over all ranks of `group`.
+
+    `local` is this rank's [nr][k] tensor of sums for its contiguous replica block
+    replica_block(R, world, rank) (nr = its size, 0 allowed).  Returns the [R][k] FP64 tensor, on
+    local's device, of every replica's sums on every rank: one all-reduce in which each slot has a
+    single non-zero contributor, so each replica's sums arrive bit for bit."""
+    rank, world = _world(group)
+    r0, r1 = replica_block(R, world, rank)
+    local = torch.as_tensor(local, dtype=torch.float64)
+    k = local.shape[-1] if local.dim() == 2 else 1
+    full = torch.zeros((R, k), dtype=torch.float64, device=local.device)
+    if r1 > r0:
+        full[r0:r1] = local.reshape(r1 - r0, k)
+    if world > 1:
+        dist.all_reduce(full, op=dist.ReduceOp.SUM, group=group)
+    return full
+
+
 def run_qmc_sharded(pass_fn, R, eps, N0, max_doublings=20, group=None, device="cpu"):
     """Adaptive RQMC over R replicas split across the ranks of `group`.
 
@@ -58,13 +80,9 @@ def run_qmc_sharded(pass_fn, R, eps, N0, max_doublings=20, group=None, device="c
     vom, price, total, dbl = math.inf, 0.0, 0, 0
     for dbl in range(max_doublings):
         if n_per > done:
-            part = torch.zeros((R, 2), dtype=torch.float64, device=device)
-            if r1 > r0:
-                s = pass_fn(r0, r1 - r0, done, n_per - done)
-                part[r0:r1] = torch.as_tensor(s, dtype=torch.float64, device=device).reshape(r1 - r0, 2)
-            if world > 1:
-                dist.all_reduce(part, op=dist.ReduceOp.SUM, group=group)
-            acc += part
+            s = pass_fn(r0, r1 - r0, done, n_per - done) if r1 > r0 else torch.zeros((0, 2))
+            acc += combine_replica_sums(torch.as_tensor(s, dtype=torch.float64, device=device).reshape(r1 - r0, 2),
+                                        R, group)
             done = n_per
         means = (acc[:, 0] / n_per).cpu().tolist()
         mm = 0.0
@@ -101,12 +119,9 @@ def run_mlqmc_sharded(level_fn, R, eps, M=2, max_L=10, pilot_n=1000, group=None,
     E, sig2, N, off = [0.0] * nl, [0.0] * nl, [0] * nl, [0] * nl
 
     def collect(l, n):
-        part = torch.zeros((R, 4), dtype=torch.float64, device=device)
-        if r1 > r0:
-            s = level_fn(l, r0, r1 - r0, off[l], n)
-            part[r0:r1] = torch.as_tensor(s, dtype=torch.float64, device=device).reshape(r1 - r0, 4)
-        if world > 1:
-            dist.all_reduce(part, op=dist.ReduceOp.SUM, group=group)
+        s = level_fn(l, r0, r1 - r0, off[l], n) if r1 > r0 else torch.zeros((0, 4))
+        part = combine_replica_sums(torch.as_tensor(s, dtype=torch.float64, device=device).reshape(r1 - r0, 4),
+                                    R, group)
         off[l] += n
         means = (part[:, 0] / n).cpu().tolist()
         mm = 0.0

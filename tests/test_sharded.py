@@ -129,3 +129,30 @@ def test_sharded_mlqmc_equals_one_process(eng, tmp_path):
         assert got[2] == one["n_samples"] and got[3] == one["levels"]
     import oracle_py as orc
     assert abs(one["price"] - orc.bs_call(100, 100, 1, 0.05, 0.2)) < 3 * one["std_error"] + 2e-2 / np.sqrt(2)
+
+
+def _rank_combine(rank, world, port, R, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    from conftest import load_engine
+    load_engine()
+    import fdmc_b200.sharded as sh
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        r0, r1 = sh.replica_block(R, world, rank)
+        full = np.array([[1.0 / (3 + r), np.pi * (r + 1) / 7, -r / 11.0] for r in range(R)])   # every rank knows it
+        got = sh.combine_replica_sums(torch.tensor(full[r0:r1]), R)
+        np.save(os.path.join(out_dir, "combine_%d.npy" % rank), got.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("R,world", [(5, 2), (2, 3)])
+def test_combine_replica_sums_is_bit_exact(eng, tmp_path, R, world):
+    """The benchmark's per-pass exchange: each rank's block of per-replica sums (uneven blocks, and
+    an empty one when ranks outnumber replicas) becomes every replica's sums on every rank, bit for bit."""
+    mp.spawn(_rank_combine, args=(world, _free_port(), R, str(tmp_path)), nprocs=world, join=True)
+    full = np.array([[1.0 / (3 + r), np.pi * (r + 1) / 7, -r / 11.0] for r in range(R)])
+    for rank in range(world):
+        got = np.load(tmp_path / ("combine_%d.npy" % rank))
+        assert np.array_equal(got, full), (rank, got, full)
