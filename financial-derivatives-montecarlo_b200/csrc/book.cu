@@ -92,7 +92,16 @@ constexpr int kBookWarpFloats = 1024 + kBookLsFloats + kBookAssetFloats + 2 * kB
 // transpose tile after the per-warp area.  Pairing gained nothing at d = 9 and cost 4-7 % in the
 // d 5-8 class (d = 7, and d = 8 through the larger kernel), so those keep single tiles.
 __host__ __device__ constexpr bool book_pair_tiles(int d) { return d == 11 || d == 12; }
-__host__ __device__ constexpr int book_warp_floats(int cls) { return kBookWarpFloats + (cls == 2 ? 1024 : 0); }
+// After them, the Sobol start words a warp carries from group to group of a chunk (sobol_tile): one
+// 32-word slot per tile for a path's first kBookCarryTiles tiles (a chunk's later tiles walk their
+// start word), sized so that the basket classes keep three resident CTAs per SM; the single-asset
+// class carries paths of up to kBookSingleCarryTiles tiles whole.
+constexpr int kBookCarryTiles = 24;
+constexpr int kBookSingleCarryTiles = 16;
+__host__ __device__ constexpr int book_warp_floats(int cls) {
+    return kBookWarpFloats + (cls == 2 ? 1024 : 0) + 32 * kBookCarryTiles;
+}
+constexpr int kBookSingleWarpFloats = 1024 + 32 * kBookSingleCarryTiles;
 
 // A float4 of shared memory, read at every use.  The Cholesky rows are loop-invariant and the
 // compiler otherwise keeps the factor in registers across the chunk; for baskets of up to four
@@ -242,7 +251,7 @@ struct BookAcc {
 template <int D>
 __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s, const BookOptDev& o, int r,
                                            uint64_t gb, uint64_t ge, float* buf, float* Ls, double* wrec,
-                                           double* rec, int lane) {
+                                           double* rec, uint32_t* carry, int lane) {
     using P = BookPath<D>;
     constexpr int S = 32 / D, W = S * D, DP = P::DP, NS = P::NS;
     const float* bk = a.bdata + o.bsk_off;
@@ -305,10 +314,13 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
         for (uint64_t g = gb; g < ge; g++) {
             P path;
             path.init(sg);
-            for (int k0 = 0; k0 < nf; k0 += S2) {
+            for (int k0 = 0, t = 0; k0 < nf; k0 += S2, t += 2) {
                 const int dim = k0 * D + lane;
-                sobol_tile(dr, dstride, dim, dim < Dt, g, a.u_cap, buf, lane);
-                sobol_tile(dr, dstride, dim + 32, lane < W2 - 32 && dim + 32 < Dt, g, a.u_cap, buf2, lane);
+                const bool cont = g != gb;
+                sobol_tile(dr, dstride, dim, dim < Dt, g, a.u_cap, buf, lane,
+                           t < kBookCarryTiles ? carry + 32 * t + lane : nullptr, cont);
+                sobol_tile(dr, dstride, dim + 32, lane < W2 - 32 && dim + 32 < Dt, g, a.u_cap, buf2, lane,
+                           t + 1 < kBookCarryTiles ? carry + 32 * (t + 1) + lane : nullptr, cont);
                 __syncwarp();
                 const float4* rowA = reinterpret_cast<const float4*>(buf + lane * 32);
                 const float4* rowB = reinterpret_cast<const float4*>(buf2 + lane * 32);
@@ -338,9 +350,10 @@ __device__ __forceinline__ void book_chunk(const BookArgs& a, const BookSpec& s,
         for (uint64_t g = gb; g < ge; g++) {
             P path;
             path.init(sg);
-            for (int k0 = 0; k0 < nf; k0 += S) {
+            for (int k0 = 0, t = 0; k0 < nf; k0 += S, t++) {
                 const int dim = k0 * D + lane;
-                sobol_tile(dr, dstride, dim, lane < W && dim < Dt, g, a.u_cap, buf, lane);
+                sobol_tile(dr, dstride, dim, lane < W && dim < Dt, g, a.u_cap, buf, lane,
+                           t < kBookCarryTiles ? carry + 32 * t + lane : nullptr, g != gb);
                 __syncwarp();
                 // this path's row of the tile, read per step as float4 chunks (conflict-free in
                 // the swizzled layout) so that only one step's normals are live in registers
@@ -377,6 +390,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     float* buf = reinterpret_cast<float*>(smem4) + wib * book_warp_floats(CLS);
+    uint32_t* carry = reinterpret_cast<uint32_t*>(buf + book_warp_floats(CLS) - 32 * kBookCarryTiles);
     float* Ls = buf + 1024;
     double* wrec = reinterpret_cast<double*>(Ls + kBookLsFloats + kBookAssetFloats);
     const int c_end = a.hdr[kHdrChunk0 + CLS + 1];
@@ -399,10 +413,10 @@ __global__ void __launch_bounds__(kThreads, MINB) k_book(const __grid_constant__
         const uint64_t ge = min(gb + (uint64_t)s.gpc, gend);
         double* rec = a.records + (size_t)c * kBookNST;
         switch (o.d - 4 * CLS) {
-            case 1: book_chunk<4 * CLS + 1>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
-            case 2: book_chunk<4 * CLS + 2>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
-            case 3: book_chunk<4 * CLS + 3>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
-            default: book_chunk<4 * CLS + 4>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, lane); break;
+            case 1: book_chunk<4 * CLS + 1>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, carry, lane); break;
+            case 2: book_chunk<4 * CLS + 2>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, carry, lane); break;
+            case 3: book_chunk<4 * CLS + 3>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, carry, lane); break;
+            default: book_chunk<4 * CLS + 4>(a, s, o, r, gb, ge, buf, Ls, wrec, rec, carry, lane); break;
         }
     }
 }
@@ -417,12 +431,13 @@ __device__ __forceinline__ void single_chunk(const KParams& kp, const BookSpec& 
     Acc<C::NST> acc;
     acc.zero();
     const uint64_t pend = (uint64_t)s.offset + s.n_points;
+    uint32_t* carry = ((kp.D + 31) / 32 <= kBookSingleCarryTiles) ? reinterpret_cast<uint32_t*>(buf + 1024) : nullptr;
     for (uint64_t h = gb; h < ge; h++) {
         const uint64_t n = h * 32 + (uint64_t)lane;
         C cons;
         cons.init(kp);
         cons.bind(r, n);
-        run_group<GEN_SOBOL, NOISE_RAW>(kp, cons, dr, 0u, h, n, buf, nullptr, lane);
+        run_group<GEN_SOBOL, NOISE_RAW>(kp, cons, dr, 0u, h, n, buf, nullptr, lane, carry, h != gb);
         float y[C::NST];
         cons.finish(kp, y);
         if (n >= s.offset && n < pend) acc.add(y);
@@ -450,7 +465,7 @@ template <int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) k_book_single(const __grid_constant__ BookArgs a) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    float* buf = reinterpret_cast<float*>(smem4) + wib * 1024;
+    float* buf = reinterpret_cast<float*>(smem4) + wib * kBookSingleWarpFloats;
     const int c_end = a.hdr[kHdrChunk0 + kSingleClass + 1];
     const int s_beg = a.hdr[kHdrSlice0 + kSingleClass], s_last = a.hdr[kHdrSlice0 + kSingleClass + 1] - 1;
     for (;;) {
@@ -580,7 +595,7 @@ namespace {
 constexpr int kIterCap = 50;   // run_mlqmc_cuda's iteration cap (:1950)
 
 size_t book_smem(int cls) {
-    return (size_t)kWarpsPerBlock * (cls == kSingleClass ? 1024 : book_warp_floats(cls)) * sizeof(float);
+    return (size_t)kWarpsPerBlock * (cls == kSingleClass ? kBookSingleWarpFloats : book_warp_floats(cls)) * sizeof(float);
 }
 
 // normals a path of the option takes per step (assets of a basket, factors of a single-asset model)

@@ -335,3 +335,36 @@ def test_mixed_book_batched_equals_plain_and_black_scholes(gpu):
             assert abs(r["price"] - bs) < o.eps / math.sqrt(2) + 3 * r["std_error"], (r, bs)
             checked += 1
     assert checked >= 1
+
+
+@pytest.mark.parametrize("d,level", [(3, 3), (12, 3), (16, 6)])
+def test_book_slice_carried_start_words(gpu, orc, d, level):
+    """A slice long enough for chunks of several 32-path groups, where the book kernel carries each
+    tile's Sobol start word from group to group (a path's first 24 tiles; the d = 16 path at level 6
+    has 32, its last 8 walk theirs; d = 12 generates tile pairs): sums against the FP64 oracle."""
+    o, (S0, sig, Lc, w, K, r, T) = _basket(gpu, d, 300 + d, max_L=8)
+    ml, qc = gpu.mlmc_cfg(M=2, n0_steps=1), gpu.qmc_cfg(R=4, salt_base=42)
+    offset, N = 37, 20000
+    g = gpu.book_level_sums(o, level, offset, N, ml, qc)
+    m = gpu.basket_gbm(S0, sig, L=Lc, weights=w, mu=r, T=T)
+    p = gpu.basket(K, r, T, d)
+    ref = orc.basket_level_sums(m, p, 2 ** level, 2, salt_base=42 + level * 4, R=4, offset=offset, N=N)
+    for q in range(4):
+        scale = N + abs(ref[:, 3 if q in (1, 3) else 2]).max()
+        assert np.abs(g[:, q] - ref[:, q]).max() < 2e-5 * scale, (q, g[:, q], ref[:, q])
+
+
+@pytest.mark.parametrize("level", [4, 8, 9])
+def test_book_single_asset_carried_start_words(gpu, orc, level):
+    """Single-asset chunks of several groups carry their start words when the path has at most 16
+    tiles (Heston at level 8: 256 steps x 2 factors = 16 tiles) and walk them beyond (level 9):
+    slice sums against the FP64 oracle either way."""
+    o, m, p = _single(gpu, "heston", "lookback", max_L=10)
+    ml, qc = gpu.mlmc_cfg(M=2, n0_steps=1), gpu.qmc_cfg(R=4, salt_base=42)
+    offset, N = 37, 20000
+    g = gpu.book_level_sums(o, level, offset, N, ml, qc)
+    ref = orc.level_sums(m, p, 2 ** level, 2, None, use_sobol=True, salt_base=42 + level * 4, R=4,
+                         offset=offset, N=N)
+    for q in (0, 2):
+        scale = N + abs(ref[:, 2]).max()
+        assert np.abs(g[:, q] - ref[:, q]).max() < 2e-5 * scale, (q, g[:, q], ref[:, q])
