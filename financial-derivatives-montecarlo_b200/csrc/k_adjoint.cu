@@ -34,24 +34,33 @@ struct LvEval {
     float w00, w01, w10, w11;
 };
 
-// bilinear sigma(S, t) on the uniform grid exactly as lv_sigma, with dsigma/dS and the weights
-__device__ __forceinline__ LvEval lv_eval(const KParams& p, float S, float t) {
+// Bilinear sigma(S, t) on the uniform grid exactly as lv_sigma, with dsigma/dS and the weights.  Every
+// path of a step k shares t = k h, so the time axis comes from a per-step table: the CTA forms row
+// k = {j nK (as float bits), b} once (lv_time_row, lv_sigma's expressions) and the sweeps read it;
+// the same values, bit for bit, without the clamp, truncation and conversion of t in each of the
+// three evaluations per step.
+__device__ __forceinline__ float2 lv_time_row(const KParams& p, int k) {
+    const float t = (float)k * p.h;
+    float y = (t - p.lv_t0) * p.lv_inv_dt;
+    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
+    const int j = min((int)y, p.lv_nt - 2);
+    return make_float2(__int_as_float(j * p.lv_nK), y - (float)j);
+}
+__device__ __forceinline__ LvEval lv_eval_row(const KParams& p, float S, float2 row) {
     LvEval e;
     float x = (S - p.lv_K0) * p.lv_inv_dK;
     const bool inside = x > 0.f && x < (float)(p.lv_nK - 1);
     x = fminf(fmaxf(x, 0.f), (float)(p.lv_nK - 1));
     const int i = min((int)x, p.lv_nK - 2);
     const float a = x - (float)i;
-    float y = (t - p.lv_t0) * p.lv_inv_dt;
-    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
-    const int j = min((int)y, p.lv_nt - 2);
-    const float b = y - (float)j;
-    const float* g = p.lv + j * p.lv_nK + i;
+    const int jn = __float_as_int(row.x);
+    const float b = row.y;
+    const float* g = p.lv + jn + i;
     const float s00 = __ldg(g), s01 = __ldg(g + 1), s10 = __ldg(g + p.lv_nK), s11 = __ldg(g + p.lv_nK + 1);
     const float lo = fmaf(a, s01 - s00, s00), hi = fmaf(a, s11 - s10, s10);
     e.sig = fmaf(b, hi - lo, lo);
     e.dsig = inside ? ((1.f - b) * (s01 - s00) + b * (s11 - s10)) * p.lv_inv_dK : 0.f;
-    e.n00 = j * p.lv_nK + i;
+    e.n00 = jn + i;
     e.w00 = (1.f - a) * (1.f - b);
     e.w01 = a * (1.f - b);
     e.w10 = (1.f - a) * b;
@@ -59,10 +68,12 @@ __device__ __forceinline__ LvEval lv_eval(const KParams& p, float S, float t) {
     return e;
 }
 
-// local volatility and its S-derivative / sigma-parameter derivative for the model
+// local volatility and its S-derivative / sigma-parameter derivative for the model at step k
+// (t = k h; the grid model reads its time row from `trow`)
 template <int MOD>
-__device__ __forceinline__ float local_sigma(const KParams& p, float S, float t, float* dsig_dS,
+__device__ __forceinline__ float local_sigma(const KParams& p, float S, int k, const float2* trow, float* dsig_dS,
                                              float* dsig_dpar, LvEval* lv) {
+    const float t = (float)k * p.h;
     if constexpr (MOD == MOD_GBM) {
         *dsig_dS = 0.f;
         *dsig_dpar = 1.f;
@@ -73,7 +84,7 @@ __device__ __forceinline__ float local_sigma(const KParams& p, float S, float t,
         *dsig_dpar = sl / p.sigma0;
         return sl;
     } else {
-        *lv = lv_eval(p, S, t);
+        *lv = lv_eval_row(p, S, trow[k]);
         *dsig_dS = lv->dsig;
         *dsig_dpar = 1.f;
         return lv->sig;
@@ -90,12 +101,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
     const int per_warp = 1024 + n_ck * 32 + kCk * 32;
     float* nodes = reinterpret_cast<float*>(smem4);               // [n_nodes] FP32, CTA-wide
     const int node_floats = (MOD == MOD_LVGRID) ? ((p.lv_nK * p.lv_nt + 3) & ~3) : 0;
-    float* wbase = nodes + node_floats + wib * per_warp;
+    const int trow_floats = (MOD == MOD_LVGRID) ? ((2 * (N + 1) + 3) & ~3) : 0;
+    float2* trow = reinterpret_cast<float2*>(nodes + node_floats);   // [N + 1] time rows (grid model)
+    float* wbase = nodes + node_floats + trow_floats + wib * per_warp;
     float* buf = wbase;               // 32 x 32 transpose tile
     float* ck = wbase + 1024;         // checkpoints [n_ck][32]
     float* seg = ck + n_ck * 32;      // recomputed segment [CK][32]
     if constexpr (MOD == MOD_LVGRID) {
         for (int i = threadIdx.x; i < node_floats; i += blockDim.x) nodes[i] = 0.f;
+        for (int k = threadIdx.x; k <= N; k += blockDim.x) trow[k] = lv_time_row(p, k);
         __syncthreads();
     }
     const float h = p.h, sqh = p.sqrt_h, muh = p.mu * p.h;
@@ -133,7 +147,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                         if ((i & (kCk - 1)) == 0) ck[(k / kCk) * 32 + lane] = S;
                         float dsS, dsP;
                         LvEval lv;
-                        const float sig = local_sigma<MOD>(p, S, (float)k * h, &dsS, &dsP, &lv);
+                        const float sig = local_sigma<MOD>(p, S, k, trow, &dsS, &dsP, &lv);
                         S = fmaf(S, fmaf(sig, zc[q] * sqh, muh), S);
                         if constexpr (PAY == PAY_ASIAN) ts += S;
                         if constexpr (PAY == PAY_LOOKBACK) {
@@ -182,7 +196,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                             seg[i * 32 + lane] = Sr;
                             float dsS, dsP;
                             LvEval lv;
-                            const float sig = local_sigma<MOD>(p, Sr, (float)(k0 + i) * h, &dsS, &dsP, &lv);
+                            const float sig = local_sigma<MOD>(p, Sr, k0 + i, trow, &dsS, &dsP, &lv);
                             Sr = fmaf(Sr, fmaf(sig, zc[q] * sqh, muh), Sr);
                         }
                     }
@@ -198,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
                             const float dw = zc[q] * sqh;
                             float dsS, dsP;
                             LvEval lv;
-                            const float sig = local_sigma<MOD>(p, Sk, (float)k * h, &dsS, &dsP, &lv);
+                            const float sig = local_sigma<MOD>(p, Sk, k, trow, &dsS, &dsP, &lv);
                             mubar = fmaf(Sbar, Sk * h, mubar);
                             const float sens = Sbar * Sk * dw;     // dP/dsigma_k through this step
                             sigbar = fmaf(sens, dsP, sigbar);
@@ -424,7 +438,8 @@ size_t adjoint_smem_bytes(int model, int n_steps, int n_nodes, int variant) {
     const int ck = kCkVariants[(variant >= 0 && variant < 3) ? variant : 0];
     const int n_ck = n_steps / ck + 1;
     const size_t per_warp = (size_t)(1024 + n_ck * 32 + ck * 32) * sizeof(float);
-    return (size_t)((n_nodes + 3) & ~3) * sizeof(float) + kWarpsPerBlock * per_warp;
+    const size_t trow = (model == MOD_LVGRID) ? (size_t)((2 * (n_steps + 1) + 3) & ~3) * sizeof(float) : 0;
+    return (size_t)((n_nodes + 3) & ~3) * sizeof(float) + trow + kWarpsPerBlock * per_warp;
 }
 
 }  // namespace mcq
