@@ -104,6 +104,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
     const int trow_floats = (MOD == MOD_LVGRID) ? ((2 * (N + 1) + 3) & ~3) : 0;
     float2* trow = reinterpret_cast<float2*>(nodes + node_floats);   // [N + 1] time rows (grid model)
     float* wbase = nodes + node_floats + trow_floats + wib * per_warp;
+    // each tile's Sobol start word, carried from group to group by the forward sweep and reused
+    // as is by the reverse sweep's regeneration of the same tile: slot 32 t + lane, after the warps
+    uint32_t* carry = reinterpret_cast<uint32_t*>(nodes + node_floats + trow_floats + kWarpsPerBlock * per_warp) +
+                      wib * N;
     float* buf = wbase;               // 32 x 32 transpose tile
     float* ck = wbase + 1024;         // checkpoints [n_ck][32]
     float* seg = ck + n_ck * 32;      // recomputed segment [CK][32]
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             float S = p.S0, ts = 0.f, tot = 0.f, comp = 0.f, mn = p.S0;
             int kmin = 0;
             for (int d0 = 0; d0 < N; d0 += 32) {
-                sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
+                sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane, carry + d0 + lane, hg != gb ? 1 : 0);
                 __syncwarp();
                 // the step loops read this lane's row of the tile from shared memory, four steps
                 // per float4 (the swizzled layout makes row reads conflict-free), and stay rolled
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_adjoint(const __grid_constant__
             int vcell = -1;
             float v00 = 0.f, v01 = 0.f, v10 = 0.f, v11 = 0.f;
             for (int d0 = N - 32; d0 >= 0; d0 -= 32) {
-                sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane);
+                sobol_tile(dr, N, d0 + lane, true, hg, p.u_cap, buf, lane, carry + d0 + lane, 2);
                 __syncwarp();
                 const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
 #pragma unroll 1
@@ -439,7 +443,8 @@ size_t adjoint_smem_bytes(int model, int n_steps, int n_nodes, int variant) {
     const int n_ck = n_steps / ck + 1;
     const size_t per_warp = (size_t)(1024 + n_ck * 32 + ck * 32) * sizeof(float);
     const size_t trow = (model == MOD_LVGRID) ? (size_t)((2 * (n_steps + 1) + 3) & ~3) * sizeof(float) : 0;
-    return (size_t)((n_nodes + 3) & ~3) * sizeof(float) + trow + kWarpsPerBlock * per_warp;
+    const size_t carry = (size_t)kWarpsPerBlock * n_steps * sizeof(uint32_t);   // start-word slots
+    return (size_t)((n_nodes + 3) & ~3) * sizeof(float) + trow + kWarpsPerBlock * per_warp + carry;
 }
 
 }  // namespace mcq

@@ -102,9 +102,10 @@ __device__ __forceinline__ void read_row(const float* buf, int lane, float (&z)[
 // The start word x(32h) = shift ^ XOR of v_k over the set bits k of gray(32h), and
 // gray(32h) = gray(h) << 5 | (h & 1) << 4, so a tile walks popcount(gray(h)) words from the
 // digital shift.  A caller that generates the same dimension for groups h - 1, h, h + 1, ... in
-// order keeps the start word of each tile in `slot` (shared memory) and passes cont = true from
-// the second group on: x(32h) = x(32(h - 1)) ^ v_4 ^ v_{5 + ctz(h)}, two words instead of the
-// walk and its chain of dependent loads (the same word, so the same normals).
+// order keeps the start word of each tile in `slot` (shared memory) and passes cont = 1 from the
+// second group on: x(32h) = x(32(h - 1)) ^ v_4 ^ v_{5 + ctz(h)}, two words instead of the walk and
+// its chain of dependent loads (the same word, so the same normals).  cont = 2: the slot already
+// holds x(32h) (a tile generated again for the same group, as the adjoint's reverse sweep does).
 //
 // The 32 points run as four blocks of eight: inside a block the gray-code step is fixed (word
 // ctz(i + 1), gray_word8), between blocks (points 8, 16, 24) it XORs word 3 + ctz(b + 1).  UNR
@@ -124,14 +125,16 @@ __device__ __forceinline__ void sobol_block8(uint32_t& x, int b, uint32_t L0, ui
 template <int UNR = 1>
 __device__ __forceinline__ void sobol_tile(const uint32_t* __restrict__ dr, int D, int dim,
                                            bool active, uint64_t h, float u_cap, float* buf,
-                                           int lane, uint32_t* slot = nullptr, bool cont = false) {
+                                           int lane, uint32_t* slot = nullptr, int cont = 0) {
     static_assert(UNR == 1 || UNR == 2 || UNR == 4, "blocks unrolled: 1, 2 or 4");
     if (!active) return;
     const uint32_t* col = dr + dim;
     const uint32_t L0 = __ldg(col), L1 = __ldg(col + D), L2 = __ldg(col + 2 * D),
                    L3 = __ldg(col + 3 * D), L4 = __ldg(col + 4 * D);
     uint32_t x;
-    if (slot != nullptr && cont) {
+    if (slot != nullptr && cont == 2) {
+        x = *slot;
+    } else if (slot != nullptr && cont) {
         x = *slot ^ L4 ^ __ldg(col + (4 + __ffsll((long long)h)) * D);
     } else {
         x = __ldg(col + 32 * D);
