@@ -378,8 +378,10 @@ int mcq_pca_matrix(mcq_handle pca, float* M_colmajor_f32);
 int mcq_debug_pass_dump(const mcq_model* m, int n_steps, int noise_mode, mcq_handle bb,
                         int use_sobol, uint32_t seed, uint32_t salt_base, int R, uint32_t offset,
                         int64_t n_points, int flags, float* out_host);
-/* Work layout of the last fused pass this process launched: the 32-point groups per work item and the Sobol start words each warp carries from group to
-   group in shared memory (0: every tile walks its start word from the digital shift). */
+/* Work layout of the last fused path-kernel launch of the allocating passes and drivers (not the
+   tensor-core PCA pass, the book or mcq_qmc_pass_noalloc): the 32-point groups per work item and
+   the Sobol start words each warp carries from group to group in shared memory (0: every tile
+   walks its start word from the digital shift). */
 int mcq_debug_last_pass_layout(int* groups_per_item, int* carry_words);
 /* The book kernel's per-replica sums over one slice of one option (level `level`, points
    offset .. offset + n_points - 1, R = qc->R replicas with salts qc->salt_base + level R + r):
