@@ -404,6 +404,35 @@ def book_slice(spec):
                                      "normals": normals, "seconds": best, "normals_per_s": normals / best}}))
 
 
+def pass_case(name, repeats=6):
+    """One fused pass of another benchmark configuration, `repeats` calls through the public API
+    (the profiling cases of those kernels): `heston_level` is the config-3 coupled level pair
+    (Heston kappa 2, theta 0.04, xi 0.3, rho -0.7, v0 0.04, r 0.02, Euler-Milstein variance, lookback
+    call, level 4 of M = 4 and n0 = 4: 1024 fine / 256 coarse steps, 16 replicas x 2^17 scrambled
+    points; the first three calls are the autotuner's trials); `philox_eur` is the config-1 plain MC pass (GBM European, S0 = K = 100, r 0.05,
+    sigma 0.2, 64 steps, 2^22 Philox paths)."""
+    eng = load_engine()
+    eng.init(0)
+    if name == "heston_level":
+        m = eng.heston(100.0, 0.02, 2.0, 0.04, 0.3, -0.7, 0.04, 1.0)
+        run = lambda: eng.level_pass(m, eng.lookback(0.3), 4 * 4 ** 4, 4, use_sobol=True, salt_base=42,  # noqa: E731
+                                     R=16, n_points=1 << 17, flags=eng.FLAG_HESTON_MILSTEIN)
+        units = 16 * (1 << 17) * (1024 + 256)
+    elif name == "philox_eur":
+        m = eng.gbm(100.0, 0.05, 0.2, 1.0)
+        run = lambda: eng.mc_pass(m, eng.european(100.0, 0.05, 1.0), 64, 123, 0, 0, 1 << 22)  # noqa: E731
+        units = (1 << 22) * 64
+    else:
+        raise SystemExit("unknown --pass-case " + name)
+    best = float("inf")
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        out = run()
+        best = min(best, time.perf_counter() - t0)
+    print(json.dumps({"pass_case": {"name": name, "seconds": best, "path_steps_per_s": units / best,
+                                    "sums": [float(v) for v in out.reshape(-1)[:4]]}}))
+
+
 def adjoint_case(n_points, repeats=3):
     """The config-4 adjoint (64 x 32 local-vol grid, Asian call, T 2, 512 steps, 16 replicas x
     n_points scrambled paths, price + delta + rho + 2048 node vegas), `repeats` calls through the
@@ -467,6 +496,8 @@ def main():
     ap.add_argument("--book-slice", default=None, metavar="D:LEVEL[:POINTS]",
                     help="only price one slice of a D-asset basket at LEVEL through the book kernel "
                          "(R = 16, M = 2, n0 = 1) and print its normals/s: the profiling case")
+    ap.add_argument("--pass-case", default=None, choices=["heston_level", "philox_eur"],
+                    help="only run one fused pass of another configuration (the profiling cases)")
     ap.add_argument("--adjoint-case", type=int, default=None, metavar="POINTS",
                     help="only run the config-4 local-vol adjoint with 16 x POINTS paths, three times (the "
                          "profiling case of k_adjoint)")
@@ -474,6 +505,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.adjoint_case:
         return adjoint_case(args.adjoint_case)
+    if args.pass_case:
+        return pass_case(args.pass_case)
     if args.impl == "reference":
         return run_reference(args)
     if args.book_slice:
