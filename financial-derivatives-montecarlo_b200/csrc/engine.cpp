@@ -298,15 +298,22 @@ void fill_params(Workspace& ws, const PassArgs& a, KParams& k) {
         const size_t nn = (size_t)m.lv_nK * m.lv_nt;
         std::vector<float> g(nn);
         for (size_t i = 0; i < nn; i++) g[i] = (float)m.lv_sigma[i];
-        float* d = (float*)ws.aux.ensure(nn * sizeof(float));
+        // the grid, then the time rows of the pass's fine steps (16-byte aligned)
+        const size_t grid_bytes = (nn * sizeof(float) + 15) & ~(size_t)15;
+        const int n_rows = a.n_steps + 1;
+        char* d = (char*)ws.aux.ensure(grid_bytes + (size_t)n_rows * sizeof(float2));
         MCQ_CUDA(cudaMemcpyAsync(d, g.data(), nn * sizeof(float), cudaMemcpyHostToDevice, ws.stream));
-        k.lv = d;
+        k.lv = (const float*)d;
         k.lv_nK = m.lv_nK;
         k.lv_nt = m.lv_nt;
         k.lv_K0 = (float)K0;
         k.lv_inv_dK = (float)iK;
         k.lv_t0 = (float)t0;
         k.lv_inv_dt = (float)it;
+        float2* rows = (float2*)(d + grid_bytes);
+        launch_lv_rows(k, rows, n_rows, ws.stream);
+        engine().launches++;
+        k.lv_rows = rows;
     }
 }
 

@@ -34,18 +34,10 @@ struct LvEval {
     float w00, w01, w10, w11;
 };
 
-// Bilinear sigma(S, t) on the uniform grid exactly as lv_sigma, with dsigma/dS and the weights.  Every
-// path of a step k shares t = k h, so the time axis comes from a per-step table: the CTA forms row
-// k = {j nK (as float bits), b} once (lv_time_row, lv_sigma's expressions) and the sweeps read it;
-// the same values, bit for bit, without the clamp, truncation and conversion of t in each of the
-// three evaluations per step.
-__device__ __forceinline__ float2 lv_time_row(const KParams& p, int k) {
-    const float t = (float)k * p.h;
-    float y = (t - p.lv_t0) * p.lv_inv_dt;
-    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
-    const int j = min((int)y, p.lv_nt - 2);
-    return make_float2(__int_as_float(j * p.lv_nK), y - (float)j);
-}
+// Bilinear sigma(S, t) on the uniform grid exactly as the pricing pass's lv_sigma_row, with dsigma/dS
+// and the weights.  The time axis comes from the same per-step rows {j nK (as float bits), b}
+// (lv_time_row, path_kernels.cuh), which the CTA forms once in shared memory; the sweeps read them
+// instead of clamping, truncating and converting t in each of the three evaluations per step.
 __device__ __forceinline__ LvEval lv_eval_row(const KParams& p, float S, float2 row) {
     LvEval e;
     float x = (S - p.lv_K0) * p.lv_inv_dK;

@@ -106,4 +106,14 @@ void launch_wait_probe(int* err, uint32_t polls, cudaStream_t s) {
     k_wait_probe<<<1, 32, 0, s>>>(err, polls);
 }
 
+// Time rows of the grid local-vol model for steps 0 .. n - 1 of a pass (lv_time_row).
+__global__ void k_lv_rows(const __grid_constant__ KParams p, float2* rows, int n) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        rows[k] = lv_time_row(p, k);
+}
+
+void launch_lv_rows(const KParams& p, float2* rows, int n, cudaStream_t s) {
+    k_lv_rows<<<(n + 255) / 256, 256, 0, s>>>(p, rows, n);
+}
+
 }  // namespace mcq

@@ -86,6 +86,7 @@ struct KParams {
     const float* bsk;
     // ---- local-vol grid sigma[j * nK + i], uniform axes
     const float* lv;
+    const float2* lv_rows;   // [n_steps + 1] time rows of the fine steps (lv_time_row)
     int lv_nK, lv_nt;
     float lv_K0, lv_inv_dK, lv_t0, lv_inv_dt;
     // ---- Brownian bridge, one row per Sobol dimension j (= bb_precompute step j):

@@ -255,16 +255,25 @@ struct AccWarp {
 
 // ------------------------------------------------------------------ models and payoffs
 
-__device__ __forceinline__ float lv_sigma(const KParams& p, float S, float t) {
+// Grid local volatility, bilinear in (S, t) on the uniform axes.  Every path of a step k shares
+// t = k h, so the time axis comes from a per-step row {j nK (as float bits), b} that the engine forms
+// once per pass (k_lv_rows) with these expressions; the paths then read it instead of clamping,
+// truncating and converting t at every step (the same values, bit for bit).
+__device__ __forceinline__ float2 lv_time_row(const KParams& p, int k) {
+    const float t = (float)k * p.h;
+    float y = (t - p.lv_t0) * p.lv_inv_dt;
+    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
+    const int j = min((int)y, p.lv_nt - 2);
+    return make_float2(__int_as_float(j * p.lv_nK), y - (float)j);
+}
+
+__device__ __forceinline__ float lv_sigma_row(const KParams& p, float S, float2 row) {
     float x = (S - p.lv_K0) * p.lv_inv_dK;
     x = fminf(fmaxf(x, 0.f), (float)(p.lv_nK - 1));
     const int i = min((int)x, p.lv_nK - 2);
     const float a = x - (float)i;
-    float y = (t - p.lv_t0) * p.lv_inv_dt;
-    y = fminf(fmaxf(y, 0.f), (float)(p.lv_nt - 1));
-    const int j = min((int)y, p.lv_nt - 2);
-    const float b = y - (float)j;
-    const float* g = p.lv + j * p.lv_nK + i;
+    const float b = row.y;
+    const float* g = p.lv + __float_as_int(row.x) + i;
     const float s00 = __ldg(g), s01 = __ldg(g + 1), s10 = __ldg(g + p.lv_nK),
                 s11 = __ldg(g + p.lv_nK + 1);
     const float lo = fmaf(a, s01 - s00, s00), hi = fmaf(a, s11 - s10, s10);
@@ -333,16 +342,17 @@ struct Leg {
         else if constexpr (PAY == PAY_LOOKBACK || PAY == PAY_DOWNOUT) r0 = on ? fminf(r0, S) : r0;
         else if constexpr (PAY == PAY_UPOUT) r0 = on ? fmaxf(r0, S) : r0;
     }
+    // t = ks h is step ks's time (the grid local-vol model reads its time row ks instead)
     template <bool RUN>
     __device__ __forceinline__ void step(const KParams& p, float dw1, float dw2, float t,
-                                         float muh, float omk, float hstep) {
+                                         float muh, float omk, float hstep, int ks) {
         if constexpr (MOD == MOD_GBM) {
             S = fmaf(S, fmaf(p.sigma, dw1, muh), S);
         } else if constexpr (MOD == MOD_DUPIRE) {
             const float sl = dupire_vol(p, S * p.inv_S0, t);
             S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_LVGRID) {
-            const float sl = lv_sigma(p, S, t);
+            const float sl = lv_sigma_row(p, S, __ldg(p.lv_rows + ks));
             S = fmaf(S, fmaf(sl, dw1, muh), S);
         } else if constexpr (MOD == MOD_HESTON) {
             // S + S (mu h + sqrt(V+) dW1): the drift joins the random increment before the one
@@ -411,10 +421,10 @@ struct PathC {
     __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
         const float t = (float)k * p.h;
         if constexpr (HES && COUPLED) {   // run_upd is a runtime flag only here
-            f.template step<false>(p, dw1, dw2, t, muh_f, p.om_f, p.h);
+            f.template step<false>(p, dw1, dw2, t, muh_f, p.om_f, p.h, k);
             if constexpr (path_dep<PAY>()) f.update_if(run_upd);
         } else {
-            f.template step<true>(p, dw1, dw2, t, muh_f, p.om_f, p.h);
+            f.template step<true>(p, dw1, dw2, t, muh_f, p.om_f, p.h, k);
         }
         k++;
         if constexpr (COUPLED) {
@@ -423,10 +433,10 @@ struct PathC {
             if (++m == p.M) {
                 const float tc = (float)ck * p.hc;
                 if constexpr (HES) {
-                    c.template step<false>(p, a1, a2, tc, muh_c, p.om_c, p.hc);
+                    c.template step<false>(p, a1, a2, tc, muh_c, p.om_c, p.hc, ck);
                     if constexpr (path_dep<PAY>()) c.update_if(run_upd);
                 } else {
-                    c.template step<true>(p, a1, a2, tc, muh_c, p.om_c, p.hc);
+                    c.template step<true>(p, a1, a2, tc, muh_c, p.om_c, p.hc, ck);
                 }
                 a1 = a2 = 0.f; m = 0; ck++;
             }
