@@ -404,6 +404,8 @@ struct Leg {
 // Single-level / coupled fine-coarse path (kernel_mc, kernel_mlmc).
 template <int MOD, int PAY, bool COUPLED>
 struct PathC {
+    // the grid local-vol time rows are those of the fine steps (a coarse leg would need its own)
+    static_assert(!(COUPLED && MOD == MOD_LVGRID), "no coupled grid local-vol pass");
     static constexpr int NST = COUPLED ? 4 : 2;
     __device__ __forceinline__ void bind(int, uint64_t) {}
     static constexpr bool HES = (MOD == MOD_HESTON);
