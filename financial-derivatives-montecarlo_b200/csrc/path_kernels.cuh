@@ -420,7 +420,8 @@ struct PathC {
         run_upd = !(HES && COUPLED && (p.flags & 2));
         if constexpr (COUPLED) { c.init(p); a1 = a2 = 0.f; m = 0; ck = 0; muh_c = p.mu * p.hc; }
     }
-    __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
+    // one fine step and, coupled, its increments summed for the coarse step
+    __device__ __forceinline__ void fine_dw(const KParams& p, float dw1, float dw2) {
         const float t = (float)k * p.h;
         if constexpr (HES && COUPLED) {   // run_upd is a runtime flag only here
             f.template step<false>(p, dw1, dw2, t, muh_f, p.om_f, p.h, k);
@@ -432,22 +433,78 @@ struct PathC {
         if constexpr (COUPLED) {
             a1 += dw1;
             if constexpr (HES) a2 += dw2;
+        }
+    }
+    // the coarse step on the last M fine increments
+    __device__ __forceinline__ void coarse_now(const KParams& p) {
+        const float tc = (float)ck * p.hc;
+        if constexpr (HES) {
+            c.template step<false>(p, a1, a2, tc, muh_c, p.om_c, p.hc, ck);
+            if constexpr (path_dep<PAY>()) c.update_if(run_upd);
+        } else {
+            c.template step<true>(p, a1, a2, tc, muh_c, p.om_c, p.hc, ck);
+        }
+        a1 = a2 = 0.f; ck++;
+    }
+    __device__ __forceinline__ void step_dw(const KParams& p, float dw1, float dw2) {
+        fine_dw(p, dw1, dw2);
+        if constexpr (COUPLED) {
             if (++m == p.M) {
-                const float tc = (float)ck * p.hc;
-                if constexpr (HES) {
-                    c.template step<false>(p, a1, a2, tc, muh_c, p.om_c, p.hc, ck);
-                    if constexpr (path_dep<PAY>()) c.update_if(run_upd);
-                } else {
-                    c.template step<true>(p, a1, a2, tc, muh_c, p.om_c, p.hc, ck);
-                }
-                a1 = a2 = 0.f; m = 0; ck++;
+                coarse_now(p);
+                m = 0;
+            }
+        }
+    }
+    // A full tile of a coupled pair with M = MM fine steps per coarse step, entered with no fine
+    // step pending (m = 0, which holds at every tile boundary when M divides the tile's steps): the
+    // coarse steps fall on compile-time positions instead of a counter test per fine step (the same
+    // steps in the same order, so the same bits).
+    template <int MM>
+    __device__ __forceinline__ void tile_mm(const KParams& p, const float (&z)[32]) {
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            fine_dw(p, z[i] * p.sqrt_h, 0.f);
+            if ((i % MM) == MM - 1) coarse_now(p);
+        }
+    }
+    template <int MM>
+    __device__ __forceinline__ void tile_hes_mm(const KParams& p, const float (&z)[32]) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const float z1 = z[2 * i], z2 = z[2 * i + 1];
+            fine_dw(p, z1 * p.sqrt_h, fmaf(p.L10, z1, p.L11 * z2) * p.sqrt_h);
+            if ((i % MM) == MM - 1) coarse_now(p);
+        }
+    }
+    template <int MM>
+    __device__ __forceinline__ void tile_smem_mm(const KParams& p, const float4* row4, int lane) {
+#pragma unroll 1
+        for (int c2 = 0; c2 < 4; c2++) {
+#pragma unroll
+            for (int cc = 0; cc < 2; cc++) {
+                const float4 v = row4[(2 * c2 + cc) ^ (lane & 7)];
+                fine_dw(p, v.x * p.sqrt_h, fmaf(p.L10, v.x, p.L11 * v.y) * p.sqrt_h);
+                fine_dw(p, v.z * p.sqrt_h, fmaf(p.L10, v.z, p.L11 * v.w) * p.sqrt_h);
+                if (MM == 2 || cc == 1) coarse_now(p);   // after fine steps 2 (M = 2) or 4 (M = 4)
             }
         }
     }
     // raw normals, tile of 32 dimensions starting at a tile boundary
     __device__ __forceinline__ void tile(const KParams& p, const float (&z)[32], int nv) {
         if (nv == 32) {
-            if constexpr (HES) {
+            if constexpr (HES && COUPLED) {
+                if (m == 0 && p.M == 2) {
+                    tile_hes_mm<2>(p, z);
+                } else if (m == 0 && p.M == 4) {
+                    tile_hes_mm<4>(p, z);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; i++) {
+                        const float z1 = z[2 * i], z2 = z[2 * i + 1];
+                        step_dw(p, z1 * p.sqrt_h, fmaf(p.L10, z1, p.L11 * z2) * p.sqrt_h);
+                    }
+                }
+            } else if constexpr (HES) {
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
                     const float z1 = z[2 * i], z2 = z[2 * i + 1];
@@ -458,6 +515,15 @@ struct PathC {
 #pragma unroll
                 for (int i = 0; i < 32; i++) f.step_gbm_z(z[i], sig_sqh, muh_f);
                 k += 32;
+            } else if constexpr (COUPLED) {
+                if (m == 0 && p.M == 2) {
+                    tile_mm<2>(p, z);
+                } else if (m == 0 && p.M == 4) {
+                    tile_mm<4>(p, z);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; i++) step_dw(p, z[i] * p.sqrt_h, 0.f);
+                }
             } else {
 #pragma unroll
                 for (int i = 0; i < 32; i++) step_dw(p, z[i] * p.sqrt_h, 0.f);
@@ -484,6 +550,14 @@ struct PathC {
     static constexpr bool SMEM_TILE = HES;
     __device__ __forceinline__ void tile_smem(const KParams& p, const float* buf, int lane, int nv) {
         const float4* row4 = reinterpret_cast<const float4*>(buf + lane * 32);
+        if constexpr (COUPLED) {
+            if (nv == 32 && m == 0 && (p.M == 2 || p.M == 4)) {
+                if (p.M == 2) tile_smem_mm<2>(p, row4, lane);
+                else tile_smem_mm<4>(p, row4, lane);
+                flush();
+                return;
+            }
+        }
 #pragma unroll 2
         for (int c = 0; c < 8; c++) {
             if (4 * c < nv) {
